@@ -1,0 +1,777 @@
+// backend.cu — create / step / transfer logic of the B200 FDM stepper.
+//
+// Behaviour mirrors the reference backend's C ABI contract
+// (native/backends/fdm/src/api.cpp:87-376, context.cu:377-1316) and the CPU
+// engine's step semantics (crates/fullmag-engine/src/lib.rs:1217-1249 Heun,
+// 1412-1568 DP45).  Differences by design:
+//   - one arena allocation per handle, one non-blocking stream, no blocking
+//     device-wide syncs except the single stats read-back per step;
+//   - the RHS at the accepted state is kept (k1 cache), so a Heun step costs
+//     two demag evaluations instead of three and a rejected DP45 attempt does
+//     not recompute stage 1;
+//   - DP45's error max-norm is reduced on the device (FP64), not on the host.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "backend.hpp"
+#include "backend_impl.hpp"
+#include "demag.cuh"
+#include "newell_host.hpp"
+#include "stages.cuh"
+
+namespace fm {
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+bool cuda_ok(Backend &b, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return true;
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "CUDA error in %s: %s (%d)", what, cudaGetErrorString(e), (int)e);
+    b.last_error = buf;
+    return false;
+}
+
+static bool check_launch(Backend &b, const char *what) {
+    return cuda_ok(b, cudaGetLastError(), what);
+}
+
+bool make_line_plan(int L, LinePlan &p) {
+    p.L = L;
+    p.nstages = 0;
+    int m = L;
+    while (m % 4 == 0 && m > 1) { p.radix[p.nstages++] = 4; m /= 4; }
+    while (m % 2 == 0 && m > 1) { p.radix[p.nstages++] = 2; m /= 2; }
+    for (int r : {3, 5, 7})
+        while (m % r == 0 && m > 1) {
+            if (p.nstages >= kMaxStages) return false;
+            p.radix[p.nstages++] = r;
+            m /= r;
+        }
+    return m == 1;
+}
+
+// Timing of one launch group (extension API: per-kernel device time).
+struct ProfScope {
+    Backend &b;
+    int id = -1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ProfScope(Backend &b_, const char *name) : b(b_) {
+        if (!b.profiling) return;
+        for (size_t i = 0; i < b.prof_names.size(); ++i)
+            if (b.prof_names[i] == name) { id = (int)i; break; }
+        if (id < 0) {
+            id = (int)b.prof_names.size();
+            b.prof_names.emplace_back(name);
+            b.prof_ms.push_back(0.0);
+            b.prof_count.push_back(0);
+        }
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, b.stream);
+    }
+    ~ProfScope() {
+        if (!b.profiling || id < 0) return;
+        cudaEventRecord(e1, b.stream);
+        b.prof_pending.push_back({id, {e0, e1}});
+    }
+};
+
+void prof_collect(Backend &b) {
+    for (auto &p : b.prof_pending) {
+        float ms = 0.f;
+        cudaEventSynchronize(p.second.second);
+        cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+        b.prof_ms[p.first] += ms;
+        b.prof_count[p.first] += 1;
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    b.prof_pending.clear();
+}
+
+// ---------------------------------------------------------------------------
+// typed implementation
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Impl {
+    using C = cx<T>;
+
+    static DemagArgs<T> demag_args(Backend &b, const void *m, void *hd) {
+        DemagArgs<T> a{};
+        a.nx = b.nx; a.ny = b.ny; a.nz = b.nz; a.n = b.n;
+        a.Lx = b.Lx; a.Ly = b.Ly; a.Lz = b.Lz; a.nkx = b.nkx;
+        a.KZ = b.KZ; a.KY = b.KY;
+        a.px = b.px; a.py = b.py; a.pz = b.pz;
+        a.twx = (const C *)b.twx; a.twy = (const C *)b.twy; a.twz = (const C *)b.twz;
+        a.s1 = (C *)b.s1; a.s2 = (C *)b.s2;
+        a.spec = (const T *)b.spec;
+        a.m = (const T *)m;
+        a.mask = b.d_mask;
+        a.ms_map = b.d_msmap;
+        a.ms = b.ms;
+        a.hd = (T *)hd;
+        a.norm = 1.0 / ((double)b.Lx * (double)b.Ly * (double)b.Lz);
+        a.lines_x = b.lines_x; a.lines_y = b.lines_y; a.kt_z = b.kt_z; a.kb_y = b.kb_y;
+        return a;
+    }
+
+    static bool configure(Backend &b) {
+        const int budget = 100 * 1024;
+        const int sz = (int)sizeof(C);
+        auto lines_for = [&](int ld, int L, int per_line_mult, int maxl) {
+            int avail = budget - L * sz;
+            int l = avail / (2 * ld * sz * per_line_mult);
+            return std::max(1, std::min(maxl, l));
+        };
+        b.lines_x = lines_for(b.Lx + 3, b.Lx, 1, 8);
+        b.smem_xf = (size_t)sz * (b.Lx + 2 * (size_t)b.lines_x * (b.Lx + 3));
+        if (b.thin) {
+            b.kb_y = lines_for(b.Ly + 1, b.Ly, 3, 8);
+            b.kb_y = std::min(b.kb_y, b.nkx);
+            b.smem_yc = (size_t)sz * (b.Ly + 2 * 3 * (size_t)b.kb_y * (b.Ly + 1));
+        } else {
+            b.lines_y = lines_for(b.Ly + 1, b.Ly, 1, 16);
+            b.smem_yf = (size_t)sz * (b.Ly + 2 * (size_t)b.lines_y * (b.Ly + 1));
+            b.kt_z = lines_for(b.Lz + 1, b.Lz, 3, 32);
+            b.kt_z = std::min(b.kt_z, b.Ly);
+            b.smem_z = (size_t)sz * (b.Lz + 2 * 3 * (size_t)b.kt_z * (b.Lz + 1));
+        }
+        const size_t maxs = 227 * 1024;
+        if (b.smem_xf > maxs || b.smem_yf > maxs || b.smem_z > maxs || b.smem_yc > maxs) {
+            b.last_error = "padded FFT length too large for the shared-memory FFT (max 4096 per axis)";
+            return false;
+        }
+        bool ok = true;
+        ok &= cuda_ok(b, cudaFuncSetAttribute(k_x_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.smem_xf), "attr x_fwd");
+        ok &= cuda_ok(b, cudaFuncSetAttribute(k_x_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.smem_xf), "attr x_inv");
+        if (b.thin) {
+            ok &= cuda_ok(b, cudaFuncSetAttribute(k_y_conv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.smem_yc), "attr y_conv");
+        } else {
+            ok &= cuda_ok(b, cudaFuncSetAttribute(k_y_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.smem_yf), "attr y_fwd");
+            ok &= cuda_ok(b, cudaFuncSetAttribute(k_y_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.smem_yf), "attr y_inv");
+            ok &= cuda_ok(b, cudaFuncSetAttribute(k_z_conv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.smem_z), "attr z_conv");
+        }
+        return ok;
+    }
+
+    // H_d(m) into hd.
+    static bool demag(Backend &b, const void *m, void *hd) {
+        if (!b.enable_demag) return true;
+        DemagArgs<T> a = demag_args(b, m, hd);
+        const int RB = 2 * b.lines_x;
+        dim3 gx((b.ny + RB - 1) / RB, b.nz, 3);
+        {
+            ProfScope p(b, "demag_x_fwd");
+            k_x_fwd<T><<<gx, 256, b.smem_xf, b.stream>>>(a);
+        }
+        if (b.thin) {
+            ProfScope p(b, "demag_y_conv");
+            k_y_conv<T><<<(b.nkx + b.kb_y - 1) / b.kb_y, 256, b.smem_yc, b.stream>>>(a);
+        } else {
+            const long long lines = 3LL * b.nz * b.nkx;
+            const unsigned gy = (unsigned)((lines + b.lines_y - 1) / b.lines_y);
+            {
+                ProfScope p(b, "demag_y_fwd");
+                k_y_fwd<T><<<gy, 256, b.smem_yf, b.stream>>>(a);
+            }
+            {
+                ProfScope p(b, "demag_z_conv");
+                dim3 gz((b.Ly + b.kt_z - 1) / b.kt_z, b.nkx);
+                k_z_conv<T><<<gz, 256, b.smem_z, b.stream>>>(a);
+            }
+            {
+                ProfScope p(b, "demag_y_inv");
+                k_y_inv<T><<<gy, 256, b.smem_yf, b.stream>>>(a);
+            }
+        }
+        {
+            ProfScope p(b, "demag_x_inv");
+            k_x_inv<T><<<gx, 256, b.smem_xf, b.stream>>>(a);
+        }
+        return check_launch(b, "demag");
+    }
+
+    static StageArgs<T> stage_args(Backend &b, const void *m, double t) {
+        StageArgs<T> s{};
+        s.nx = b.nx; s.ny = b.ny; s.nz = b.nz; s.n = b.n;
+        s.idx2 = (T)(1.0 / (b.dx * b.dx));
+        s.idy2 = (T)(1.0 / (b.dy * b.dy));
+        s.idz2 = (T)(1.0 / (b.dz * b.dz));
+        s.dinv[0] = 1.0 / (b.dx * b.dx);
+        s.dinv[1] = 1.0 / (b.dy * b.dy);
+        s.dinv[2] = 1.0 / (b.dz * b.dz);
+        s.aex = b.aex; s.ms = b.ms; s.ms_map = b.d_msmap;
+        s.mask = b.d_mask; s.region = b.d_region; s.lut = b.d_lut;
+        s.enable_exchange = b.enable_exchange; s.enable_demag = b.enable_demag;
+        s.has_ext = b.has_ext;
+        for (int c = 0; c < 3; ++c) { s.hext[c] = b.hext[c]; s.hac[c] = b.hac[c]; }
+        s.ac_omega = 2.0 * kPi * b.ac_freq;
+        s.gamma_bar = b.gamma / (1.0 + b.alpha * b.alpha);
+        s.alpha = b.alpha;
+        s.precession = b.precession;
+        s.vol = b.dx * b.dy * b.dz;
+        s.t = t;
+        s.m = (const T *)m;
+        s.hd = (const T *)b.hd;
+        return s;
+    }
+
+    static unsigned grid_cells(const Backend &b) {
+        return (unsigned)std::min<long long>((b.n + 255) / 256, (long long)b.red_blocks);
+    }
+
+    // k = RHS(m, t); optional observables and diagnostics.
+    static bool eval(Backend &b, const void *m, double t, void *kout, bool diag, bool obs) {
+        StageArgs<T> s = stage_args(b, m, t);
+        s.kout = (T *)kout;
+        s.hex_out = obs ? (T *)b.hex : nullptr;
+        s.heff_out = obs ? (T *)b.heff : nullptr;
+        s.partials = diag ? b.partials : nullptr;
+        const unsigned g = diag ? (unsigned)b.red_blocks : grid_cells(b);
+        {
+            ProfScope p(b, "stage_eval");
+            k_stage<T, MODE_EVAL><<<g, 256, 0, b.stream>>>(s);
+        }
+        if (diag) {
+            ProfScope p(b, "reduce_finalize");
+            k_finalize<<<1, 256, 0, b.stream>>>(b.partials, b.red_blocks, b.d_out);
+        }
+        return check_launch(b, "stage_eval");
+    }
+
+    static bool combine(Backend &b, int form, const void *m0, std::initializer_list<void *> ks,
+                        std::initializer_list<double> cs, double dt, void *out) {
+        CombineArgs<T> a{};
+        a.n = b.n;
+        a.m0 = (const T *)m0;
+        int i = 0;
+        for (void *k : ks) a.k[i++] = (const T *)k;
+        i = 0;
+        for (double c : cs) a.c[i++] = c;
+        a.dt = dt;
+        a.form = form;
+        a.out = (T *)out;
+        {
+            ProfScope p(b, "stage_combine");
+            k_combine<T><<<grid_cells(b), 256, 0, b.stream>>>(a);
+        }
+        return check_launch(b, "combine");
+    }
+
+    static bool read_stats(Backend &b) {
+        if (!cuda_ok(b, cudaMemcpyAsync(b.h_out, b.d_out, NQ * sizeof(double), cudaMemcpyDeviceToHost, b.stream), "stats D2H"))
+            return false;
+        return cuda_ok(b, cudaStreamSynchronize(b.stream), "stats sync");
+    }
+
+    static void fill_stats(Backend &b, double dt, fullmag_fdm_step_stats *st) {
+        const double *o = b.h_out;
+        st->step = b.step_count;
+        st->time_seconds = b.time;
+        st->dt_seconds = dt;
+        st->exchange_energy_joules = b.enable_exchange ? o[Q_EEX] : 0.0;
+        st->demag_energy_joules = b.enable_demag ? o[Q_EDEMAG] : 0.0;
+        st->external_energy_joules = b.has_ext ? o[Q_EEXT] : 0.0;
+        st->total_energy_joules =
+            st->exchange_energy_joules + st->demag_energy_joules + st->external_energy_joules;
+        st->max_effective_field_amplitude = std::sqrt(o[Q_HEFF2]);
+        st->max_demag_field_amplitude = b.enable_demag ? std::sqrt(o[Q_HD2]) : 0.0;
+        st->max_rhs_amplitude = std::sqrt(o[Q_RHS2]);
+    }
+
+    static bool ensure_k1(Backend &b) {
+        if (b.k1_valid) return true;
+        if (!demag(b, b.m, b.hd)) return false;
+        if (!eval(b, b.m, b.time, b.k[0], false, false)) return false;
+        b.k1_valid = true;
+        return true;
+    }
+
+    // One Heun step (lib.rs:1217-1249) with the cached k1.
+    static bool heun(Backend &b, double dt, fullmag_fdm_step_stats *st, bool readback) {
+        if (!ensure_k1(b)) return false;
+        // predictor m_p = normalize(m + k1 dt)
+        if (!combine(b, 0, b.m, {b.k[0]}, {dt}, dt, b.mstage)) return false;
+        if (!demag(b, b.mstage, b.hd)) return false;
+        // corrector at m_p: k2 and m <- normalize(m0 + (k1 + k2) dt/2)
+        StageArgs<T> s = stage_args(b, b.mstage, b.time + dt);
+        s.kout = (T *)b.k[1];
+        s.m0 = (T *)b.m;
+        s.k1 = (const T *)b.k[0];
+        s.half_dt = 0.5 * dt;
+        {
+            ProfScope p(b, "stage_heun_corr");
+            k_stage<T, MODE_HEUN_CORR><<<grid_cells(b), 256, 0, b.stream>>>(s);
+        }
+        if (!check_launch(b, "heun corrector")) return false;
+        // fields, RHS (next k1) and diagnostics at the new state
+        if (!demag(b, b.m, b.hd)) return false;
+        if (!eval(b, b.m, b.time + dt, b.k[0], true, false)) return false;
+        b.time += dt;
+        b.step_count += 1;
+        b.k1_valid = true;
+        b.obs_valid = false;
+        if (readback) {
+            if (!read_stats(b)) return false;
+            fill_stats(b, dt, st);
+            st->suggested_next_dt = 0.0;
+        }
+        return true;
+    }
+
+    // One accepted DP45 step (lib.rs:1412-1568).
+    static bool dp45(Backend &b, double dt_in, fullmag_fdm_step_stats *st) {
+        const double A21 = 1.0 / 5.0;
+        const double A31 = 3.0 / 40.0, A32 = 9.0 / 40.0;
+        const double A41 = 44.0 / 45.0, A42 = -56.0 / 15.0, A43 = 32.0 / 9.0;
+        const double A51 = 19372.0 / 6561.0, A52 = -25360.0 / 2187.0, A53 = 64448.0 / 6561.0,
+                     A54 = -212.0 / 729.0;
+        const double A61 = 9017.0 / 3168.0, A62 = -355.0 / 33.0, A63 = 46732.0 / 5247.0,
+                     A64 = 49.0 / 176.0, A65 = -5103.0 / 18656.0;
+        const double B1 = 35.0 / 384.0, B3 = 500.0 / 1113.0, B4 = 125.0 / 192.0,
+                     B5 = -2187.0 / 6784.0, B6 = 11.0 / 84.0;
+        // initial dt clamped like rk45_step_buf (lib.rs:1419): min(dt_max) then max(dt_min)
+        double dt = std::max(std::min(dt_in, b.dt_max), b.dt_min);
+        if (!ensure_k1(b)) return false;
+        void **k = b.k;
+        for (;;) {
+            const double t = b.time;
+            if (!combine(b, 0, b.m, {k[0]}, {A21 * dt}, dt, b.mstage)) return false;
+            if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + 0.2 * dt, k[1], false, false)) return false;
+            if (!combine(b, 1, b.m, {k[0], k[1]}, {A31, A32}, dt, b.mstage)) return false;
+            if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + 0.3 * dt, k[2], false, false)) return false;
+            if (!combine(b, 2, b.m, {k[0], k[1], k[2]}, {A41, A42, A43}, dt, b.mstage)) return false;
+            if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + 0.8 * dt, k[3], false, false)) return false;
+            if (!combine(b, 3, b.m, {k[0], k[1], k[2], k[3]}, {A51, A52, A53, A54}, dt, b.mstage)) return false;
+            if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + 8.0 / 9.0 * dt, k[4], false, false)) return false;
+            if (!combine(b, 4, b.m, {k[0], k[1], k[2], k[3], k[4]}, {A61, A62, A63, A64, A65}, dt, b.mstage)) return false;
+            if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + dt, k[5], false, false)) return false;
+            // 5th-order solution and k7 = RHS(y5) with the embedded error norm
+            if (!combine(b, 4, b.m, {k[0], k[2], k[3], k[4], k[5]}, {B1, B3, B4, B5, B6}, dt, b.mstage)) return false;
+            if (!demag(b, b.mstage, b.hd)) return false;
+            StageArgs<T> s = stage_args(b, b.mstage, t + dt);
+            s.kout = (T *)k[6];
+            s.partials = b.partials;
+            s.ke[0] = (const T *)k[0]; s.ke[1] = (const T *)k[2]; s.ke[2] = (const T *)k[3];
+            s.ke[3] = (const T *)k[4]; s.ke[4] = (const T *)k[5];
+            s.dt = dt;
+            {
+                ProfScope p(b, "stage_dp45_last");
+                k_stage<T, MODE_DP45_LAST><<<b.red_blocks, 256, 0, b.stream>>>(s);
+            }
+            {
+                ProfScope p(b, "reduce_finalize");
+                k_finalize<<<1, 256, 0, b.stream>>>(b.partials, b.red_blocks, b.d_out);
+            }
+            if (!check_launch(b, "dp45 last stage") || !read_stats(b)) return false;
+            const double err = std::sqrt(b.h_out[Q_ERR2]);
+            if (err <= b.max_error || dt <= b.dt_min) {
+                std::swap(b.m, b.mstage);
+                std::swap(k[0], k[6]);  // FSAL: k7 is the next step's k1
+                b.time += dt;
+                b.step_count += 1;
+                b.k1_valid = true;
+                b.obs_valid = false;
+                fill_stats(b, dt, st);
+                st->suggested_next_dt = std::min(
+                    std::max(b.headroom * dt * std::pow(b.max_error / std::max(err, 1e-30), 0.2), b.dt_min),
+                    b.dt_max);
+                return true;
+            }
+            const double dt_new = b.headroom * dt * std::pow(b.max_error / err, 0.2);
+            dt = std::min(std::max(dt_new, b.dt_min), b.dt_max);
+            // k[0] still equals RHS(m0, t): nothing to recompute for stage 1
+        }
+    }
+
+    static bool refresh(Backend &b) {
+        if (!demag(b, b.m, b.hd)) return false;
+        if (!eval(b, b.m, b.time, b.k[0], false, true)) return false;
+        b.k1_valid = true;
+        b.obs_valid = true;
+        return cuda_ok(b, cudaStreamSynchronize(b.stream), "refresh");
+    }
+
+    static bool ensure_obs(Backend &b) {
+        if (b.obs_valid) return true;
+        // hd holds H_d(m) after a step; recompute H_ex / H_eff (and k1, unchanged)
+        if (!eval(b, b.m, b.time, b.k[0], false, true)) return false;
+        b.obs_valid = true;
+        return true;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// AoS <-> SoA conversion kernels
+// ---------------------------------------------------------------------------
+template <typename TI, typename TO>
+__global__ void k_aos_to_soa(const TI *in, TO *out, long long n, const uint8_t *mask,
+                             const double *ms_map) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        bool act = (!mask || mask[i] != 0) && (!ms_map || ms_map[i] > 0.0);
+        out[i] = act ? (TO)in[3 * i] : TO(0);
+        out[n + i] = act ? (TO)in[3 * i + 1] : TO(0);
+        out[2 * n + i] = act ? (TO)in[3 * i + 2] : TO(0);
+    }
+}
+
+template <typename TI, typename TO>
+__global__ void k_soa_to_aos(const TI *in, TO *out, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        out[3 * i] = (TO)in[i];
+        out[3 * i + 1] = (TO)in[n + i];
+        out[3 * i + 2] = (TO)in[2 * n + i];
+    }
+}
+
+// Box average of the preview bins, same binning as the reference
+// (native/backends/fdm/src/context.cu:222-286).
+template <typename TI, typename TO>
+__global__ void k_preview(const TI *f, long long n, int fx, int fy, int fz, int px, int py,
+                          int pz, int z_origin, int z_stride, TO *out) {
+    const long long count = (long long)px * py * pz;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < count;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int ix = (int)(p % px), iy = (int)((p / px) % py), iz = (int)(p / ((long long)px * py));
+        int x0 = (int)(((long long)ix * fx) / px), x1 = (int)(((long long)(ix + 1) * fx) / px);
+        if (x1 <= x0) x1 = x0 + 1;
+        if (x1 > fx) x1 = fx;
+        int y0 = (int)(((long long)iy * fy) / py), y1 = (int)(((long long)(iy + 1) * fy) / py);
+        if (y1 <= y0) y1 = y0 + 1;
+        if (y1 > fy) y1 = fy;
+        long long zs = (long long)z_origin + (long long)iz * z_stride;
+        if (zs >= fz) zs = fz - 1;
+        long long ze = (long long)z_origin + (long long)(iz + 1) * z_stride;
+        if (ze <= zs) ze = zs + 1;
+        if (ze > fz) ze = fz;
+        double ax = 0, ay = 0, az = 0, cnt = 0;
+        for (long long z = zs; z < ze; ++z)
+            for (int y = y0; y < y1; ++y)
+                for (int x = x0; x < x1; ++x) {
+                    const long long i = (z * fy + y) * fx + x;
+                    ax += (double)f[i];
+                    ay += (double)f[n + i];
+                    az += (double)f[2 * n + i];
+                    cnt += 1.0;
+                }
+        out[3 * p] = (TO)(ax / cnt);
+        out[3 * p + 1] = (TO)(ay / cnt);
+        out[3 * p + 2] = (TO)(az / cnt);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// public (C++) entry points used by api.cu
+// ---------------------------------------------------------------------------
+static unsigned cgrid(long long n) {
+    return (unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 16));
+}
+
+bool backend_alloc(Backend &b) {
+    const bool dbl = b.precision == FULLMAG_FDM_PRECISION_DOUBLE;
+    b.scalar = dbl ? 8 : 4;
+    const size_t cs = 2 * b.scalar;  // complex
+    const size_t vec = (size_t)3 * b.n * b.scalar;
+    // layout sizes
+    struct Item { void **p; size_t bytes; };
+    std::vector<Item> items;
+    const int nk = b.integrator == FULLMAG_FDM_INTEGRATOR_DP45 ? 7 : 2;
+    items.push_back({&b.m, vec});
+    items.push_back({&b.mstage, vec});
+    items.push_back({&b.hd, vec});
+    items.push_back({&b.hex, vec});
+    items.push_back({&b.heff, vec});
+    for (int i = 0; i < nk; ++i) items.push_back({&b.k[i], vec});
+    if (b.enable_demag) {
+        items.push_back({&b.twx, (size_t)b.Lx * cs});
+        items.push_back({&b.twy, (size_t)b.Ly * cs});
+        items.push_back({&b.twz, (size_t)b.Lz * cs});
+        items.push_back({&b.s1, (size_t)3 * b.nz * b.nkx * b.ny * cs});
+        if (!b.thin) items.push_back({&b.s2, (size_t)3 * b.nz * b.nkx * b.Ly * cs});
+        items.push_back({&b.spec, (size_t)6 * b.KZ * b.nkx * b.KY * b.scalar});
+    }
+    items.push_back({&b.staging, (size_t)3 * b.n * sizeof(double)});
+    if (b.has_mask) items.push_back({(void **)&b.d_mask, (size_t)b.n});
+    if (b.has_regions) {
+        items.push_back({(void **)&b.d_region, (size_t)b.n * 4});
+        items.push_back({(void **)&b.d_lut, (size_t)256 * 256 * 8});
+    }
+    if (b.has_ms_map) items.push_back({(void **)&b.d_msmap, (size_t)b.n * 8});
+    b.red_blocks = (int)std::max<long long>(1, std::min<long long>((b.n + 255) / 256, 148LL * 8));
+    items.push_back({(void **)&b.partials, (size_t)NQ * b.red_blocks * 8});
+    items.push_back({(void **)&b.d_out, (size_t)NQ * 8 + 64});
+    size_t total = 0;
+    for (auto &it : items) total += (it.bytes + 255) / 256 * 256;
+    if (!cuda_ok(b, cudaMalloc(&b.arena, total), "cudaMalloc(arena)")) return false;
+    b.arena_bytes = total;
+    char *p = (char *)b.arena;
+    for (auto &it : items) {
+        *it.p = p;
+        p += (it.bytes + 255) / 256 * 256;
+    }
+    if (!cuda_ok(b, cudaMemsetAsync(b.arena, 0, total, b.stream), "arena memset")) return false;
+    if (!cuda_ok(b, cudaMallocHost((void **)&b.h_out, NQ * sizeof(double) + 64), "cudaMallocHost(stats)")) return false;
+    return true;
+}
+
+template <typename T>
+static bool upload_tables(Backend &b, const std::vector<double> (&spec)[6]) {
+    auto tw = [&](int L, void *dst) {
+        std::vector<cx<T>> t(L);
+        for (int k = 0; k < L; ++k) {
+            const double a = 2.0 * kPi * (double)k / (double)L;
+            t[k] = mk<T>((T)std::cos(a), (T)(-std::sin(a)));
+        }
+        return cuda_ok(b, cudaMemcpy(dst, t.data(), L * sizeof(cx<T>), cudaMemcpyHostToDevice), "twiddles");
+    };
+    if (!tw(b.Lx, b.twx) || !tw(b.Ly, b.twy) || !tw(b.Lz, b.twz)) return false;
+    const size_t plane = (size_t)b.KZ * b.nkx * b.KY;
+    std::vector<T> host(6 * plane);
+    for (int c = 0; c < 6; ++c)
+        for (size_t o = 0; o < plane; ++o) host[c * plane + o] = (T)spec[c][o];
+    return cuda_ok(b, cudaMemcpy(b.spec, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice), "spectra upload");
+}
+
+bool backend_upload_tables(Backend &b, const std::vector<double> (&spec)[6]) {
+    if (!b.enable_demag) return true;
+    return b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? upload_tables<double>(b, spec)
+                                                       : upload_tables<float>(b, spec);
+}
+
+bool backend_configure(Backend &b) {
+    if (!b.enable_demag) return true;
+    return b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::configure(b)
+                                                       : Impl<float>::configure(b);
+}
+
+template <typename TI>
+static bool upload_m_impl(Backend &b, const TI *host, uint64_t len) {
+    if (!cuda_ok(b, cudaMemcpyAsync(b.staging, host, len * sizeof(TI), cudaMemcpyHostToDevice, b.stream), "upload m"))
+        return false;
+    if (b.precision == FULLMAG_FDM_PRECISION_DOUBLE)
+        k_aos_to_soa<TI, double><<<cgrid(b.n), 256, 0, b.stream>>>((const TI *)b.staging, (double *)b.m, b.n, b.d_mask, b.d_msmap);
+    else
+        k_aos_to_soa<TI, float><<<cgrid(b.n), 256, 0, b.stream>>>((const TI *)b.staging, (float *)b.m, b.n, b.d_mask, b.d_msmap);
+    if (!check_launch(b, "aos_to_soa")) return false;
+    b.k1_valid = false;
+    b.obs_valid = false;
+    return cuda_ok(b, cudaStreamSynchronize(b.stream), "upload sync");
+}
+
+bool backend_upload_m_f64(Backend &b, const double *m, uint64_t len) { return upload_m_impl<double>(b, m, len); }
+bool backend_upload_m_f32(Backend &b, const float *m, uint64_t len) { return upload_m_impl<float>(b, m, len); }
+
+bool backend_refresh(Backend &b) {
+    return b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::refresh(b) : Impl<float>::refresh(b);
+}
+
+bool backend_step(Backend &b, double dt, fullmag_fdm_step_stats *st) {
+    bool ok;
+    if (b.integrator == FULLMAG_FDM_INTEGRATOR_DP45)
+        ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::dp45(b, dt, st) : Impl<float>::dp45(b, dt, st);
+    else
+        ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::heun(b, dt, st, true)
+                                                         : Impl<float>::heun(b, dt, st, true);
+    if (b.profiling) prof_collect(b);
+    return ok;
+}
+
+bool backend_step_n(Backend &b, double dt, uint32_t nsteps, fullmag_fdm_step_stats *st) {
+    bool ok = true;
+    for (uint32_t i = 0; i < nsteps && ok; ++i) {
+        const bool last = (i + 1 == nsteps);
+        if (b.integrator == FULLMAG_FDM_INTEGRATOR_DP45) {
+            ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::dp45(b, dt, st) : Impl<float>::dp45(b, dt, st);
+            if (ok) dt = st->suggested_next_dt;
+        } else {
+            ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::heun(b, dt, st, last)
+                                                             : Impl<float>::heun(b, dt, st, last);
+        }
+    }
+    if (b.profiling) prof_collect(b);
+    return ok;
+}
+
+// Field pointer for an observable (after making H_ex / H_eff current).
+static const void *observable_ptr(Backend &b, fullmag_fdm_observable obs, bool &ok) {
+    ok = true;
+    switch (obs) {
+        case FULLMAG_FDM_OBSERVABLE_M: return b.m;
+        case FULLMAG_FDM_OBSERVABLE_H_DEMAG: return b.hd;
+        case FULLMAG_FDM_OBSERVABLE_H_EX:
+        case FULLMAG_FDM_OBSERVABLE_H_EFF:
+            ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::ensure_obs(b) : Impl<float>::ensure_obs(b);
+            return obs == FULLMAG_FDM_OBSERVABLE_H_EX ? b.hex : b.heff;
+        default: ok = false; return nullptr;
+    }
+}
+
+// Host-side H_ext value of cell i (synthesised like context.cu:802-815).
+static void hext_cell(const Backend &b, long long i, double out[3]) {
+    const bool act = (!b.has_mask || b.mask_host[i] != 0) && (!b.has_ms_map || b.ms_map_host[i] > 0.0);
+    const double s = (b.ac_freq != 0.0) ? std::sin(2.0 * kPi * b.ac_freq * b.time) : 0.0;
+    for (int c = 0; c < 3; ++c) out[c] = (b.has_ext && act) ? b.hext[c] + b.hac[c] * s : 0.0;
+}
+
+template <typename TO>
+static bool download_impl(Backend &b, fullmag_fdm_observable obs, TO *out, uint64_t len) {
+    if (obs == FULLMAG_FDM_OBSERVABLE_H_EXT) {
+        for (long long i = 0; i < b.n; ++i) {
+            double h[3];
+            hext_cell(b, i, h);
+            out[3 * i] = (TO)h[0]; out[3 * i + 1] = (TO)h[1]; out[3 * i + 2] = (TO)h[2];
+        }
+        return true;
+    }
+    bool ok;
+    const void *src = observable_ptr(b, obs, ok);
+    if (!ok) {
+        if (b.last_error.empty()) b.last_error = "unsupported observable";
+        return false;
+    }
+    if (b.precision == FULLMAG_FDM_PRECISION_DOUBLE)
+        k_soa_to_aos<double, TO><<<cgrid(b.n), 256, 0, b.stream>>>((const double *)src, (TO *)b.staging, b.n);
+    else
+        k_soa_to_aos<float, TO><<<cgrid(b.n), 256, 0, b.stream>>>((const float *)src, (TO *)b.staging, b.n);
+    if (!check_launch(b, "soa_to_aos")) return false;
+    if (!cuda_ok(b, cudaMemcpyAsync(out, b.staging, len * sizeof(TO), cudaMemcpyDeviceToHost, b.stream), "field D2H"))
+        return false;
+    return cuda_ok(b, cudaStreamSynchronize(b.stream), "field sync");
+}
+
+bool backend_download_f64(Backend &b, fullmag_fdm_observable o, double *out, uint64_t len) { return download_impl<double>(b, o, out, len); }
+bool backend_download_f32(Backend &b, fullmag_fdm_observable o, float *out, uint64_t len) { return download_impl<float>(b, o, out, len); }
+
+template <typename TO>
+static bool preview_impl(Backend &b, fullmag_fdm_observable obs, uint32_t pnx, uint32_t pny,
+                         uint32_t pnz, uint32_t z_origin, uint32_t z_stride, TO *out, uint64_t len) {
+    if (z_origin >= (uint32_t)b.nz) { b.last_error = "preview z_origin out of range"; return false; }
+    if ((int)pnx == b.nx && (int)pny == b.ny && (int)pnz == b.nz && z_origin == 0 && z_stride == 1)
+        return download_impl<TO>(b, obs, out, len);
+    const long long count = (long long)pnx * pny * pnz;
+    if (obs == FULLMAG_FDM_OBSERVABLE_H_EXT) {
+        // fraction of active cells in the bin times H_ext (context.cu:941-1000)
+        for (long long p = 0; p < count; ++p) {
+            const int ix = (int)(p % pnx), iy = (int)((p / pnx) % pny), iz = (int)(p / ((long long)pnx * pny));
+            int x0 = (int)(((long long)ix * b.nx) / pnx), x1 = (int)(((long long)(ix + 1) * b.nx) / pnx);
+            if (x1 <= x0) x1 = x0 + 1;
+            if (x1 > b.nx) x1 = b.nx;
+            int y0 = (int)(((long long)iy * b.ny) / pny), y1 = (int)(((long long)(iy + 1) * b.ny) / pny);
+            if (y1 <= y0) y1 = y0 + 1;
+            if (y1 > b.ny) y1 = b.ny;
+            long long zs = (long long)z_origin + (long long)iz * z_stride;
+            if (zs >= b.nz) zs = b.nz - 1;
+            long long ze = (long long)z_origin + (long long)(iz + 1) * z_stride;
+            if (ze <= zs) ze = zs + 1;
+            if (ze > b.nz) ze = b.nz;
+            double act = 0, cnt = 0;
+            for (long long z = zs; z < ze; ++z)
+                for (int y = y0; y < y1; ++y)
+                    for (int x = x0; x < x1; ++x) {
+                        const long long i = (z * b.ny + y) * b.nx + x;
+                        act += ((!b.has_mask || b.mask_host[i]) && (!b.has_ms_map || b.ms_map_host[i] > 0)) ? 1.0 : 0.0;
+                        cnt += 1.0;
+                    }
+            const double sc = (b.has_ext && cnt > 0) ? act / cnt : 0.0;
+            const double s = (b.ac_freq != 0.0) ? std::sin(2.0 * kPi * b.ac_freq * b.time) : 0.0;
+            for (int c = 0; c < 3; ++c) out[3 * p + c] = (TO)((b.hext[c] + b.hac[c] * s) * sc);
+        }
+        return true;
+    }
+    bool ok;
+    const void *src = observable_ptr(b, obs, ok);
+    if (!ok) {
+        if (b.last_error.empty()) b.last_error = "unsupported observable";
+        return false;
+    }
+    if ((uint64_t)count * 3 * sizeof(TO) > (uint64_t)3 * b.n * sizeof(double)) {
+        b.last_error = "preview larger than the field";
+        return false;
+    }
+    if (b.precision == FULLMAG_FDM_PRECISION_DOUBLE)
+        k_preview<double, TO><<<cgrid(count), 256, 0, b.stream>>>((const double *)src, b.n, b.nx, b.ny, b.nz, pnx, pny, pnz, z_origin, z_stride, (TO *)b.staging);
+    else
+        k_preview<float, TO><<<cgrid(count), 256, 0, b.stream>>>((const float *)src, b.n, b.nx, b.ny, b.nz, pnx, pny, pnz, z_origin, z_stride, (TO *)b.staging);
+    if (!check_launch(b, "preview")) return false;
+    if (!cuda_ok(b, cudaMemcpyAsync(out, b.staging, count * 3 * sizeof(TO), cudaMemcpyDeviceToHost, b.stream), "preview D2H"))
+        return false;
+    return cuda_ok(b, cudaStreamSynchronize(b.stream), "preview sync");
+}
+
+bool backend_preview_f64(Backend &b, fullmag_fdm_observable o, uint32_t a, uint32_t c, uint32_t d, uint32_t zo, uint32_t zs, double *out, uint64_t len) {
+    return preview_impl<double>(b, o, a, c, d, zo, zs, out, len);
+}
+bool backend_preview_f32(Backend &b, fullmag_fdm_observable o, uint32_t a, uint32_t c, uint32_t d, uint32_t zo, uint32_t zs, float *out, uint64_t len) {
+    return preview_impl<float>(b, o, a, c, d, zo, zs, out, len);
+}
+
+// Snapshot: D2D copy on the compute stream, D2H on its own stream into pinned memory.
+bool backend_snapshot_begin(Backend &b, fullmag_fdm_observable obs, Snapshot &s) {
+    s.scalar = b.scalar;
+    s.cell_count = (uint64_t)b.n;
+    s.bytes = (size_t)3 * b.n * b.scalar;
+    if (!cuda_ok(b, cudaMallocHost(&s.host, s.bytes), "cudaMallocHost(snapshot)")) return false;
+    if (obs == FULLMAG_FDM_OBSERVABLE_H_EXT) {
+        for (long long i = 0; i < b.n; ++i) {
+            double h[3];
+            hext_cell(b, i, h);
+            for (int c = 0; c < 3; ++c) {
+                if (b.scalar == 8) ((double *)s.host)[c * b.n + i] = h[c];
+                else ((float *)s.host)[c * b.n + i] = (float)h[c];
+            }
+        }
+        s.pending = false;
+        return true;
+    }
+    bool ok;
+    const void *src = observable_ptr(b, obs, ok);
+    if (!ok) {
+        if (b.last_error.empty()) b.last_error = "unsupported async snapshot observable";
+        return false;
+    }
+    if (!cuda_ok(b, cudaMalloc(&s.dev, s.bytes), "cudaMalloc(snapshot)")) return false;
+    if (!cuda_ok(b, cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "snapshot stream")) return false;
+    if (!cuda_ok(b, cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming), "snapshot event")) return false;
+    if (!cuda_ok(b, cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming), "snapshot event")) return false;
+    if (!cuda_ok(b, cudaMemcpyAsync(s.dev, src, s.bytes, cudaMemcpyDeviceToDevice, b.stream), "snapshot D2D")) return false;
+    if (!cuda_ok(b, cudaEventRecord(s.ready, b.stream), "snapshot record")) return false;
+    if (!cuda_ok(b, cudaStreamWaitEvent(s.stream, s.ready, 0), "snapshot wait")) return false;
+    if (!cuda_ok(b, cudaMemcpyAsync(s.host, s.dev, s.bytes, cudaMemcpyDeviceToHost, s.stream), "snapshot D2H")) return false;
+    if (!cuda_ok(b, cudaEventRecord(s.done, s.stream), "snapshot record")) return false;
+    s.device = b.device;
+    s.pending = true;
+    return true;
+}
+
+void snapshot_free(Snapshot &s) {
+    if (s.done) cudaEventDestroy(s.done);
+    if (s.ready) cudaEventDestroy(s.ready);
+    if (s.stream) cudaStreamDestroy(s.stream);
+    if (s.dev) cudaFree(s.dev);
+    if (s.host) cudaFreeHost(s.host);
+    s = Snapshot{};
+}
+
+void backend_free(Backend &b) {
+    if (b.stream) cudaStreamSynchronize(b.stream);
+    for (auto &p : b.prof_pending) {
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    b.prof_pending.clear();
+    if (b.arena) cudaFree(b.arena);
+    b.arena = nullptr;
+    if (b.h_out) cudaFreeHost(b.h_out);
+    b.h_out = nullptr;
+    if (b.stream) cudaStreamDestroy(b.stream);
+    b.stream = nullptr;
+}
+
+}  // namespace fm

@@ -1,0 +1,87 @@
+// backend.hpp — per-handle state of the B200 FDM stepper (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "fullmag_fdm.h"
+#include "fullmag_fdm_ext.h"
+#include "fft.cuh"
+
+namespace fm {
+
+// Device buffers are typed by the stepper precision (float or double); they
+// are kept as void* here and cast in the templated implementation.
+struct Backend {
+    // ---- configuration (copied from the plan) ----
+    int nx = 0, ny = 0, nz = 0;
+    long long n = 0;
+    double dx = 0, dy = 0, dz = 0;
+    double ms = 0, aex = 0, alpha = 0, gamma = 0;
+    int precision = FULLMAG_FDM_PRECISION_DOUBLE;
+    int integrator = FULLMAG_FDM_INTEGRATOR_HEUN;
+    bool precession = true, enable_exchange = true, enable_demag = false, has_ext = false;
+    double hext[3] = {0, 0, 0};
+    double hac[3] = {0, 0, 0};
+    double ac_freq = 0.0;
+    bool has_mask = false, has_regions = false, has_ms_map = false;
+    std::vector<uint8_t> mask_host;
+    std::vector<double> ms_map_host;
+    long long active_count = 0;
+    double max_error = 1e-5, dt_min = 1e-18, dt_max = 1e-10, headroom = 0.8;
+
+    // ---- dynamic state ----
+    uint64_t step_count = 0;
+    double time = 0.0;
+    bool k1_valid = false;    // k[0] == RHS(m, time)
+    bool obs_valid = false;   // hex / heff hold H_ex(m), H_eff(m)
+
+    // ---- device resources ----
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    void *arena = nullptr;
+    size_t arena_bytes = 0;
+    size_t scalar = 8;        // bytes per state scalar
+    void *m = nullptr, *mstage = nullptr, *hd = nullptr;
+    void *k[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    void *hex = nullptr, *heff = nullptr;
+    void *staging = nullptr;  // device AoS staging (>= 3 n doubles)
+    uint8_t *d_mask = nullptr;
+    uint32_t *d_region = nullptr;
+    double *d_lut = nullptr;
+    double *d_msmap = nullptr;
+
+    // ---- demag ----
+    bool thin = false;        // 2-D (nz = 1) spectra path
+    bool projection = false;  // no spectra supplied: k k^T / k^2 tensor
+    int Lx = 0, Ly = 0, Lz = 0, nkx = 0, KZ = 0, KY = 0;
+    LinePlan px{}, py{}, pz{};
+    void *twx = nullptr, *twy = nullptr, *twz = nullptr;
+    void *s1 = nullptr, *s2 = nullptr, *spec = nullptr;
+    int lines_x = 1, lines_y = 1, kt_z = 1, kb_y = 1;
+    size_t smem_xf = 0, smem_yf = 0, smem_z = 0, smem_yc = 0;
+
+    // ---- reductions ----
+    int red_blocks = 0;
+    double *partials = nullptr;
+    double *d_out = nullptr;
+    double *h_out = nullptr;  // pinned, NQ doubles
+
+    // ---- per-kernel timing (extension API) ----
+    bool profiling = false;
+    std::vector<std::string> prof_names;
+    std::vector<double> prof_ms;
+    std::vector<uint64_t> prof_count;
+    std::vector<cudaEvent_t> prof_events;  // pool
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+
+    fullmag_fdm_device_info info{};
+    bool info_valid = false;
+    std::string last_error;
+    std::string err_buf;
+};
+
+}  // namespace fm

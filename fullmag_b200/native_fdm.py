@@ -1,0 +1,445 @@
+"""Python host binding of libfullmag_fdm.so.0 over its C ABI.
+
+Mirrors the reference's safe Rust wrapper ``NativeFdmBackend``
+(crates/fullmag-runner/src/native_fdm.rs:90-704): a plan is turned into a
+``fullmag_fdm_plan_desc``, the handle is created and its deferred error
+checked, then ``step`` / ``copy_m`` / ``copy_field`` / previews / snapshots /
+uploads go straight to the library.  Errors raise ``RunError`` with the
+library's ``last_error`` text, like the Rust ``RunError`` mapping
+(native_fdm.rs:696-704).
+
+There is no CPU fallback: loading fails loudly when the library or a CUDA
+device is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import build as _build
+
+MU0 = 4.0 * np.pi * 1e-7
+
+OK, ERR_INVALID, ERR_CUDA, ERR_INTERNAL = 0, -1, -2, -3
+PRECISION_SINGLE, PRECISION_DOUBLE = 1, 2
+HEUN, DP45, ABM3, RK4, RK23 = 1, 2, 3, 4, 5
+OBS_M, OBS_H_EX, OBS_H_DEMAG, OBS_H_EXT, OBS_H_EFF = 1, 2, 3, 4, 5
+SNAP_F32, SNAP_F64 = 1, 2
+DEMAG_FROM_PLAN, DEMAG_NEWELL = 0, 1
+MAX_EXCHANGE_REGIONS = 256
+
+_dp = C.POINTER(C.c_double)
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("nz", C.c_uint32),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double)]
+
+
+class MaterialDesc(C.Structure):
+    _fields_ = [("saturation_magnetisation", C.c_double), ("exchange_stiffness", C.c_double),
+                ("damping", C.c_double), ("gyromagnetic_ratio", C.c_double)]
+
+
+class PlanDesc(C.Structure):
+    _fields_ = [
+        ("grid", GridDesc), ("material", MaterialDesc),
+        ("precision", C.c_int), ("integrator", C.c_int),
+        ("disable_precession", C.c_int), ("enable_exchange", C.c_int),
+        ("enable_demag", C.c_int), ("has_external_field", C.c_int),
+        ("external_field_am", C.c_double * 3),
+        ("demag_kernel_xx_spectrum", _dp), ("demag_kernel_yy_spectrum", _dp),
+        ("demag_kernel_zz_spectrum", _dp), ("demag_kernel_xy_spectrum", _dp),
+        ("demag_kernel_xz_spectrum", _dp), ("demag_kernel_yz_spectrum", _dp),
+        ("demag_kernel_spectrum_len", C.c_uint64),
+        ("active_mask", C.POINTER(C.c_uint8)), ("active_mask_len", C.c_uint64),
+        ("region_mask", C.POINTER(C.c_uint32)), ("region_mask_len", C.c_uint64),
+        ("exchange_lut", _dp), ("exchange_lut_len", C.c_uint64),
+        ("boundary_correction", C.c_int), ("boundary_phi_floor", C.c_double),
+        ("boundary_delta_min", C.c_double),
+        ("volume_fraction", _dp), ("volume_fraction_len", C.c_uint64),
+        ("face_link_xp", _dp), ("face_link_xm", _dp), ("face_link_yp", _dp),
+        ("face_link_ym", _dp), ("face_link_zp", _dp), ("face_link_zm", _dp),
+        ("delta_xp", _dp), ("delta_xm", _dp), ("delta_yp", _dp),
+        ("delta_ym", _dp), ("delta_zp", _dp), ("delta_zm", _dp),
+        ("has_demag_boundary_corr", C.c_int),
+        ("demag_corr_target_idx", C.POINTER(C.c_int32)),
+        ("demag_corr_source_idx", C.POINTER(C.c_int32)),
+        ("demag_corr_tensor", _dp),
+        ("demag_corr_target_count", C.c_uint32), ("demag_corr_stencil_size", C.c_uint32),
+        ("initial_magnetization_xyz", _dp), ("initial_magnetization_len", C.c_uint64),
+        ("adaptive_max_error", C.c_double), ("adaptive_dt_min", C.c_double),
+        ("adaptive_dt_max", C.c_double), ("adaptive_headroom", C.c_double),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [("step", C.c_uint64), ("time_seconds", C.c_double), ("dt_seconds", C.c_double),
+                ("exchange_energy_joules", C.c_double), ("demag_energy_joules", C.c_double),
+                ("external_energy_joules", C.c_double), ("total_energy_joules", C.c_double),
+                ("max_effective_field_amplitude", C.c_double),
+                ("max_demag_field_amplitude", C.c_double), ("max_rhs_amplitude", C.c_double),
+                ("suggested_next_dt", C.c_double), ("wall_time_ns", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class DeviceInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 128), ("compute_capability_major", C.c_int),
+                ("compute_capability_minor", C.c_int), ("driver_version", C.c_int),
+                ("runtime_version", C.c_int)]
+
+
+class SnapshotDesc(C.Structure):
+    _fields_ = [("cell_count", C.c_uint64), ("component_count", C.c_uint32),
+                ("scalar_bytes", C.c_uint32), ("scalar_type", C.c_int)]
+
+
+class PlanExt(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("ms_map", _dp), ("ms_map_len", C.c_uint64),
+                ("ac_field_am", C.c_double * 3), ("ac_frequency_hz", C.c_double),
+                ("demag_source", C.c_int)]
+
+
+# Every function declared in include/fullmag_fdm.h and include/fullmag_fdm_ext.h.
+ABI_FUNCTIONS = (
+    "fullmag_fdm_is_available", "fullmag_fdm_backend_create", "fullmag_fdm_backend_step",
+    "fullmag_fdm_backend_copy_field_f64", "fullmag_fdm_backend_copy_field_f32",
+    "fullmag_fdm_backend_copy_field_preview_f64", "fullmag_fdm_backend_copy_field_preview_f32",
+    "fullmag_fdm_backend_begin_field_snapshot", "fullmag_fdm_field_snapshot_wait",
+    "fullmag_fdm_field_snapshot_destroy", "fullmag_fdm_backend_upload_magnetization_f64",
+    "fullmag_fdm_backend_upload_magnetization_f32", "fullmag_fdm_backend_refresh_observables",
+    "fullmag_fdm_backend_get_device_info", "fullmag_fdm_backend_last_error",
+    "fullmag_fdm_backend_destroy",
+)
+EXT_FUNCTIONS = (
+    "fullmag_fdm_backend_create_ext", "fullmag_fdm_backend_step_n",
+    "fullmag_fdm_backend_set_profiling", "fullmag_fdm_backend_profile_count",
+    "fullmag_fdm_backend_profile_entry", "fullmag_fdm_backend_profile_reset",
+    "fullmag_fdm_backend_memory_info", "fullmag_fdm_newell_spectra",
+)
+
+_lib = None
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def load_library(build_if_missing: bool = True):
+    """Load libfullmag_fdm.so.0 from the package (build it with nvcc if absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise RuntimeError(f"{path} is missing; run fullmag_b200/build.py")
+        _build.build()
+    L = C.CDLL(path)
+    vp = C.c_void_p
+    L.fullmag_fdm_is_available.restype = C.c_int
+    L.fullmag_fdm_backend_create.restype = vp
+    L.fullmag_fdm_backend_create.argtypes = [C.POINTER(PlanDesc)]
+    L.fullmag_fdm_backend_create_ext.restype = vp
+    L.fullmag_fdm_backend_create_ext.argtypes = [C.POINTER(PlanDesc), C.POINTER(PlanExt)]
+    L.fullmag_fdm_backend_step.argtypes = [vp, C.c_double, C.POINTER(StepStats)]
+    L.fullmag_fdm_backend_step_n.argtypes = [vp, C.c_double, C.c_uint32, C.POINTER(StepStats)]
+    L.fullmag_fdm_backend_copy_field_f64.argtypes = [vp, C.c_int, _dp, C.c_uint64]
+    L.fullmag_fdm_backend_copy_field_f32.argtypes = [vp, C.c_int, C.POINTER(C.c_float), C.c_uint64]
+    L.fullmag_fdm_backend_copy_field_preview_f64.argtypes = [vp, C.c_int] + [C.c_uint32] * 5 + [_dp, C.c_uint64]
+    L.fullmag_fdm_backend_copy_field_preview_f32.argtypes = [vp, C.c_int] + [C.c_uint32] * 5 + [C.POINTER(C.c_float), C.c_uint64]
+    L.fullmag_fdm_backend_begin_field_snapshot.restype = vp
+    L.fullmag_fdm_backend_begin_field_snapshot.argtypes = [vp, C.c_int]
+    L.fullmag_fdm_field_snapshot_wait.argtypes = [vp, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64), C.POINTER(SnapshotDesc)]
+    L.fullmag_fdm_field_snapshot_destroy.argtypes = [vp]
+    L.fullmag_fdm_field_snapshot_destroy.restype = None
+    L.fullmag_fdm_backend_upload_magnetization_f64.argtypes = [vp, _dp, C.c_uint64]
+    L.fullmag_fdm_backend_upload_magnetization_f32.argtypes = [vp, C.POINTER(C.c_float), C.c_uint64]
+    L.fullmag_fdm_backend_refresh_observables.argtypes = [vp]
+    L.fullmag_fdm_backend_get_device_info.argtypes = [vp, C.POINTER(DeviceInfo)]
+    L.fullmag_fdm_backend_last_error.restype = C.c_char_p
+    L.fullmag_fdm_backend_last_error.argtypes = [vp]
+    L.fullmag_fdm_backend_destroy.argtypes = [vp]
+    L.fullmag_fdm_backend_destroy.restype = None
+    L.fullmag_fdm_backend_set_profiling.argtypes = [vp, C.c_int]
+    L.fullmag_fdm_backend_profile_count.argtypes = [vp]
+    L.fullmag_fdm_backend_profile_entry.argtypes = [vp, C.c_int, C.POINTER(C.c_char_p), _dp, C.POINTER(C.c_uint64)]
+    L.fullmag_fdm_backend_profile_reset.argtypes = [vp]
+    L.fullmag_fdm_backend_profile_reset.restype = None
+    L.fullmag_fdm_backend_memory_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]
+    L.fullmag_fdm_newell_spectra.argtypes = [C.c_uint32] * 3 + [C.c_double] * 3 + [C.c_int] + [_dp] * 6
+    _lib = L
+    return L
+
+
+def is_available() -> bool:
+    return bool(load_library().fullmag_fdm_is_available())
+
+
+class RunError(RuntimeError):
+    pass
+
+
+def newell_spectra(nx: int, ny: int, nz: int, dx: float, dy: float, dz: float,
+                   thin_film_2d: bool = False):
+    """FP64 Newell spectra in the reference's interleaved complex layout (host code)."""
+    pz = 1 if (thin_film_2d and nz == 1) else 2 * nz
+    p = 4 * nx * ny * pz
+    outs = [np.zeros(2 * p) for _ in range(6)]
+    rc = load_library().fullmag_fdm_newell_spectra(nx, ny, nz, dx, dy, dz, int(thin_film_2d),
+                                                   *[o.ctypes.data_as(_dp) for o in outs])
+    if rc != OK:
+        raise RunError(f"fullmag_fdm_newell_spectra failed ({rc})")
+    return outs
+
+
+@dataclass
+class FdmPlan:
+    """The FdmPlanIR fields the reference runner maps into the plan descriptor
+    (crates/fullmag-runner/src/native_fdm.rs:90-346)."""
+    cells: Tuple[int, int, int]
+    cell_size: Tuple[float, float, float]
+    initial_magnetization: np.ndarray           # AoS [3N] or (N, 3)
+    saturation_magnetisation: float = 8.0e5
+    exchange_stiffness: float = 1.3e-11
+    damping: float = 0.02
+    gyromagnetic_ratio: float = 2.211e5
+    precision: int = PRECISION_DOUBLE
+    integrator: int = HEUN
+    pure_damping: bool = False
+    enable_exchange: bool = True
+    enable_demag: bool = True
+    external_field: Optional[Sequence[float]] = None   # A/m
+    active_mask: Optional[np.ndarray] = None
+    region_mask: Optional[np.ndarray] = None
+    exchange_lut: Optional[np.ndarray] = None
+    demag_spectra: Optional[Sequence[np.ndarray]] = None  # 6 interleaved arrays
+    adaptive: Optional[Tuple[float, float, float, float]] = None  # max_error, dt_min, dt_max, headroom
+    # extension block
+    ms_map: Optional[np.ndarray] = None
+    ac_field: Optional[Sequence[float]] = None
+    ac_frequency_hz: float = 0.0
+    demag_source: int = DEMAG_FROM_PLAN
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def cell_count(self) -> int:
+        return int(self.cells[0] * self.cells[1] * self.cells[2])
+
+    def to_desc(self) -> PlanDesc:
+        d = PlanDesc()
+        keep = self._keep = []
+        d.grid.nx, d.grid.ny, d.grid.nz = (int(c) for c in self.cells)
+        d.grid.dx, d.grid.dy, d.grid.dz = (float(c) for c in self.cell_size)
+        d.material.saturation_magnetisation = self.saturation_magnetisation
+        d.material.exchange_stiffness = self.exchange_stiffness
+        d.material.damping = self.damping
+        d.material.gyromagnetic_ratio = self.gyromagnetic_ratio
+        d.precision = self.precision
+        d.integrator = self.integrator
+        d.disable_precession = int(self.pure_damping)
+        d.enable_exchange = int(self.enable_exchange)
+        d.enable_demag = int(self.enable_demag)
+        d.has_external_field = int(self.external_field is not None)
+        for i, v in enumerate(self.external_field or (0.0, 0.0, 0.0)):
+            d.external_field_am[i] = float(v)
+        if self.demag_spectra is not None:
+            names = ("xx", "yy", "zz", "xy", "xz", "yz")
+            for nm, arr in zip(names, self.demag_spectra):
+                a = np.ascontiguousarray(arr, dtype=np.float64)
+                keep.append(a)
+                setattr(d, f"demag_kernel_{nm}_spectrum", a.ctypes.data_as(_dp))
+            d.demag_kernel_spectrum_len = int(np.asarray(self.demag_spectra[0]).size)
+        if self.active_mask is not None:
+            a = np.ascontiguousarray(self.active_mask, dtype=np.uint8)
+            keep.append(a)
+            d.active_mask = a.ctypes.data_as(C.POINTER(C.c_uint8))
+            d.active_mask_len = a.size
+        if self.region_mask is not None:
+            a = np.ascontiguousarray(self.region_mask, dtype=np.uint32)
+            keep.append(a)
+            d.region_mask = a.ctypes.data_as(C.POINTER(C.c_uint32))
+            d.region_mask_len = a.size
+        if self.exchange_lut is not None:
+            a = np.ascontiguousarray(self.exchange_lut, dtype=np.float64)
+            keep.append(a)
+            d.exchange_lut = a.ctypes.data_as(_dp)
+            d.exchange_lut_len = a.size
+        m0 = np.ascontiguousarray(self.initial_magnetization, dtype=np.float64).reshape(-1)
+        keep.append(m0)
+        d.initial_magnetization_xyz = m0.ctypes.data_as(_dp)
+        d.initial_magnetization_len = m0.size
+        if self.adaptive is not None:
+            (d.adaptive_max_error, d.adaptive_dt_min, d.adaptive_dt_max,
+             d.adaptive_headroom) = (float(v) for v in self.adaptive)
+        return d
+
+    def to_ext(self) -> Optional[PlanExt]:
+        if self.ms_map is None and self.ac_field is None and self.demag_source == DEMAG_FROM_PLAN:
+            return None
+        e = PlanExt()
+        e.struct_size = C.sizeof(PlanExt)
+        if self.ms_map is not None:
+            a = np.ascontiguousarray(self.ms_map, dtype=np.float64)
+            self._keep.append(a)
+            e.ms_map = a.ctypes.data_as(_dp)
+            e.ms_map_len = a.size
+        for i, v in enumerate(self.ac_field or (0.0, 0.0, 0.0)):
+            e.ac_field_am[i] = float(v)
+        e.ac_frequency_hz = float(self.ac_frequency_hz)
+        e.demag_source = int(self.demag_source)
+        return e
+
+
+class NativeFdmBackend:
+    """RAII handle over fullmag_fdm_backend (native_fdm.rs:90-704)."""
+
+    def __init__(self, plan: FdmPlan):
+        self._lib = load_library()
+        self.plan = plan
+        self.n = plan.cell_count
+        self.precision = plan.precision
+        desc = plan.to_desc()
+        ext = plan.to_ext()
+        self._desc = desc
+        if ext is None:
+            h = self._lib.fullmag_fdm_backend_create(C.byref(desc))
+        else:
+            self._ext = ext
+            h = self._lib.fullmag_fdm_backend_create_ext(C.byref(desc), C.byref(ext))
+        if not h:
+            raise RunError("CUDA FDM backend_create returned null")
+        err = self._lib.fullmag_fdm_backend_last_error(h)
+        if err is not None:
+            self._lib.fullmag_fdm_backend_destroy(h)
+            raise RunError(err.decode())
+        self._h = h
+
+    # -- lifecycle --
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.fullmag_fdm_backend_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != OK:
+            err = self._lib.fullmag_fdm_backend_last_error(self._h)
+            raise RunError(f"{what} failed ({rc}): {err.decode() if err else 'unknown error'}")
+
+    # -- stepping --
+    def step(self, dt: float) -> dict:
+        st = StepStats()
+        self._check(self._lib.fullmag_fdm_backend_step(self._h, dt, C.byref(st)), "step")
+        return st.as_dict()
+
+    def step_n(self, dt: float, n: int) -> dict:
+        st = StepStats()
+        self._check(self._lib.fullmag_fdm_backend_step_n(self._h, dt, n, C.byref(st)), "step_n")
+        return st.as_dict()
+
+    # -- transfers --
+    def copy_field(self, observable: int, dtype=np.float64) -> np.ndarray:
+        out = np.zeros(3 * self.n, dtype=dtype)
+        if dtype == np.float64:
+            rc = self._lib.fullmag_fdm_backend_copy_field_f64(self._h, observable, out.ctypes.data_as(_dp), out.size)
+        else:
+            rc = self._lib.fullmag_fdm_backend_copy_field_f32(
+                self._h, observable, out.ctypes.data_as(C.POINTER(C.c_float)), out.size)
+        self._check(rc, "copy_field")
+        return out
+
+    def copy_m(self) -> np.ndarray:
+        return self.copy_field(OBS_M)
+
+    def copy_preview(self, observable: int, preview: Tuple[int, int, int], z_origin: int = 0,
+                     z_stride: int = 1, dtype=np.float64) -> np.ndarray:
+        pnx, pny, pnz = preview
+        out = np.zeros(3 * pnx * pny * pnz, dtype=dtype)
+        fn = (self._lib.fullmag_fdm_backend_copy_field_preview_f64 if dtype == np.float64
+              else self._lib.fullmag_fdm_backend_copy_field_preview_f32)
+        ptr = out.ctypes.data_as(_dp if dtype == np.float64 else C.POINTER(C.c_float))
+        self._check(fn(self._h, observable, pnx, pny, pnz, z_origin, z_stride, ptr, out.size), "preview")
+        return out
+
+    def snapshot(self, observable: int) -> np.ndarray:
+        snap = self._lib.fullmag_fdm_backend_begin_field_snapshot(self._h, observable)
+        if not snap:
+            err = self._lib.fullmag_fdm_backend_last_error(self._h)
+            raise RunError(f"snapshot failed: {err.decode() if err else 'unknown'}")
+        try:
+            data = C.c_void_p()
+            nbytes = C.c_uint64()
+            desc = SnapshotDesc()
+            rc = self._lib.fullmag_fdm_field_snapshot_wait(snap, C.byref(data), C.byref(nbytes), C.byref(desc))
+            if rc != OK:
+                raise RunError(f"snapshot wait failed ({rc})")
+            dt = np.float32 if desc.scalar_type == SNAP_F32 else np.float64
+            buf = (C.c_char * nbytes.value).from_address(data.value)
+            return np.frombuffer(bytes(buf), dtype=dt).reshape(3, desc.cell_count).copy()
+        finally:
+            self._lib.fullmag_fdm_field_snapshot_destroy(snap)
+
+    def upload_m(self, m_aos: np.ndarray) -> None:
+        m = np.ascontiguousarray(m_aos).reshape(-1)
+        if m.dtype == np.float32:
+            rc = self._lib.fullmag_fdm_backend_upload_magnetization_f32(
+                self._h, m.ctypes.data_as(C.POINTER(C.c_float)), m.size)
+        else:
+            m = m.astype(np.float64, copy=False)
+            rc = self._lib.fullmag_fdm_backend_upload_magnetization_f64(self._h, m.ctypes.data_as(_dp), m.size)
+        self._check(rc, "upload_magnetization")
+
+    def refresh_observables(self) -> None:
+        self._check(self._lib.fullmag_fdm_backend_refresh_observables(self._h), "refresh_observables")
+
+    def device_info(self) -> dict:
+        info = DeviceInfo()
+        self._check(self._lib.fullmag_fdm_backend_get_device_info(self._h, C.byref(info)), "device_info")
+        return {"name": info.name.decode(), "cc": (info.compute_capability_major, info.compute_capability_minor),
+                "driver_version": info.driver_version, "runtime_version": info.runtime_version}
+
+    # -- extension: profiling / memory --
+    def set_profiling(self, on: bool) -> None:
+        self._lib.fullmag_fdm_backend_set_profiling(self._h, int(on))
+
+    def profile(self) -> dict:
+        out = {}
+        for i in range(self._lib.fullmag_fdm_backend_profile_count(self._h)):
+            name = C.c_char_p()
+            ms = C.c_double()
+            cnt = C.c_uint64()
+            self._lib.fullmag_fdm_backend_profile_entry(self._h, i, C.byref(name), C.byref(ms), C.byref(cnt))
+            out[name.value.decode()] = (ms.value, cnt.value)
+        return out
+
+    def profile_reset(self) -> None:
+        self._lib.fullmag_fdm_backend_profile_reset(self._h)
+
+    def memory_info(self) -> Tuple[int, Tuple[int, int, int]]:
+        b = C.c_uint64()
+        dims = (C.c_uint32 * 3)()
+        self._lib.fullmag_fdm_backend_memory_info(self._h, C.byref(b), dims)
+        return b.value, tuple(dims)

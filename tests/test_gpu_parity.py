@@ -1,0 +1,298 @@
+"""GPU parity: the CUDA path through the C ABI vs the FP64 oracle.
+
+Tolerances (stated per test):
+  - FP64 fields after refresh: 1e-12 relative to max |H_eff|;
+  - FP64 trajectories: max|dm| <= 1e-10 inside the predictability horizon of
+    the problem (see test_c1_sensitivity_floor_and_1000_steps: a 1-ulp change
+    of m0 in the oracle alone grows to ~3e-7 after 1000 C1 steps, so 1000-step
+    C1 parity is bounded by that floor, not by 1e-10);
+  - FP32-mixed vs FP64 oracle: max|dm| <= 1e-5 (the reference's tier-B bound,
+    native/backends/fdm/tests/tier_b_compare.cu:113-114);
+  - energies: relative 1e-9 (FP64) / 1e-4 (FP32-mixed).
+"""
+import numpy as np
+import pytest
+
+from fullmag_b200 import native_fdm as nf
+from oracle import oracle as O
+
+from gpu_helpers import MU0, c1_kwargs, make_pair, max_abs, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _energy_close(st, r, tol):
+    assert rel(st["exchange_energy_joules"], r["e_ex_pair"]) <= tol
+    assert rel(st["demag_energy_joules"], r["e_demag"]) <= tol or abs(r["e_demag"]) < 1e-30
+    assert abs(st["external_energy_joules"] - r["e_ext"]) <= tol * max(abs(r["e_total"]), abs(r["e_ext"]))
+    assert rel(st["max_effective_field_amplitude"], r["max_h_eff"]) <= tol
+    assert rel(st["max_rhs_amplitude"], r["max_rhs"]) <= tol
+
+
+def test_library_sees_b200():
+    assert nf.is_available()
+    be, _, _ = make_pair((8, 4, 1), (2e-9, 2e-9, 2e-9), demag=False)
+    info = be.device_info()
+    assert info["cc"][0] == 10, info
+
+
+def test_refresh_fields_match_oracle_c1():
+    kw = c1_kwargs()
+    be, sim, _ = make_pair(**kw)
+    obs = sim.observe()
+    scale = np.abs(obs["h_eff"]).max()
+    for o, key in ((nf.OBS_H_EX, "h_ex"), (nf.OBS_H_DEMAG, "h_demag"), (nf.OBS_H_EFF, "h_eff"),
+                   (nf.OBS_H_EXT, "h_ext")):
+        assert max_abs(be.copy_field(o), obs[key]) <= 1e-12 * scale, key
+
+
+@pytest.mark.parametrize("cells", [(16, 12, 4), (12, 10, 3), (7, 5, 2), (8, 8, 1)])
+def test_refresh_fields_match_oracle_3d(cells):
+    be, sim, _ = make_pair(cells, (2e-9, 2.5e-9, 3e-9), h_ext=(1e4, -2e4, 3e3), thin=False)
+    obs = sim.observe()
+    scale = np.abs(obs["h_eff"]).max()
+    assert max_abs(be.copy_field(nf.OBS_H_DEMAG), obs["h_demag"]) <= 1e-12 * scale
+    assert max_abs(be.copy_field(nf.OBS_H_EFF), obs["h_eff"]) <= 1e-12 * scale
+
+
+def test_c1_heun_fp64_100_steps():
+    be, sim, _ = make_pair(**c1_kwargs())
+    for _ in range(100):
+        st = be.step(1e-13)
+        r = sim.step(1e-13)
+    assert max_abs(be.copy_m(), sim.m) <= 1e-10
+    assert st["step"] == 100 and abs(st["time_seconds"] - 1e-11) < 1e-24
+    _energy_close(st, r, 1e-9)
+
+
+def test_c1_sensitivity_floor_and_1000_steps():
+    """1000 C1 steps: GPU-vs-oracle difference against the oracle's own floor."""
+    kw = c1_kwargs()
+    be, sim, m0 = make_pair(**kw)
+    rng = np.random.default_rng(1)
+    m1 = m0 * (1.0 + rng.uniform(-1, 1, m0.size) * 2.2e-16)
+    _, sim_p, _ = make_pair(**{**kw, "m0": m1})
+    for _ in range(1000):
+        st = be.step(1e-13)
+        r = sim.step(1e-13)
+        sim_p.step(1e-13)
+    floor = max_abs(sim.m, sim_p.m)
+    gpu = max_abs(be.copy_m(), sim.m)
+    print(f"C1 1000 steps: gpu-vs-oracle {gpu:.3e}, oracle 1-ulp floor {floor:.3e}")
+    assert gpu <= max(100.0 * floor, 1e-10)
+    assert rel(st["total_energy_joules"], r["e_total"]) <= 1e-3
+
+
+def test_smooth_3d_trajectory_1000_steps():
+    cells = (16, 12, 4)
+    n = 16 * 12 * 4
+    rng = np.random.default_rng(5)
+    m0 = np.tile([0.6, 0.8, 0.0], n) + 0.05 * rng.standard_normal(3 * n)
+    be, sim, _ = make_pair(cells, (2e-9, 2e-9, 2e-9), alpha=0.1, h_ext=(0, 30e-3 / MU0, 0), m0=m0)
+    for _ in range(1000):
+        st = be.step(5e-14)
+        r = sim.step(5e-14)
+    assert max_abs(be.copy_m(), sim.m) <= 1e-10
+    _energy_close(st, r, 1e-9)
+
+
+def _disk_mask(nx, ny, nz, r_out, r_in, d):
+    x = (np.arange(nx) + 0.5) * d - nx * d / 2
+    y = (np.arange(ny) + 0.5) * d - ny * d / 2
+    X, Y = np.meshgrid(x, y)
+    r2 = X ** 2 + Y ** 2
+    m2 = (r2 <= r_out ** 2) & (r2 > r_in ** 2)
+    return np.repeat(m2[None], nz, axis=0).astype(np.uint8).reshape(-1)
+
+
+def test_masked_regions_lut_fp64():
+    nx, ny, nz = 24, 20, 3
+    mask = _disk_mask(nx, ny, nz, 20e-9, 6e-9, 2e-9)
+    regions = np.where(np.arange(nx * ny * nz) % nx < nx // 2, 1, 2).astype(np.uint32)
+    lut = np.zeros((256, 256))
+    lut[1, 1] = lut[2, 2] = 1.3e-11
+    lut[1, 2] = lut[2, 1] = 0.4e-11
+    be, sim, _ = make_pair((nx, ny, nz), (2e-9, 2e-9, 2e-9), alpha=0.1, h_ext=(0, 3e4, 0),
+                           mask=mask, regions=regions, lut=lut, seed=44)
+    for _ in range(50):
+        st = be.step(5e-14)
+        r = sim.step(5e-14)
+    m = be.copy_m()
+    assert max_abs(m, sim.m) <= 1e-10
+    assert np.all(m.reshape(-1, 3)[mask == 0] == 0.0)
+    _energy_close(st, r, 1e-9)
+
+
+@pytest.mark.parametrize("cells", [(12, 10, 3), (7, 6, 1), (15, 9, 2)])
+def test_non_power_of_two_grids(cells):
+    be, sim, _ = make_pair(cells, (2e-9, 2e-9, 2.5e-9), alpha=0.2, h_ext=(2e4, 0, 0), seed=9)
+    for _ in range(20):
+        be.step(2e-14)
+        sim.step(2e-14)
+    assert max_abs(be.copy_m(), sim.m) <= 1e-10
+
+
+def test_pure_damping_fp64():
+    be, sim, _ = make_pair((16, 8, 2), (2e-9, 2e-9, 2e-9), alpha=0.5, h_ext=(0, 0, 5e4),
+                           pure_damping=True)
+    for _ in range(30):
+        be.step(1e-14)
+        sim.step(1e-14)
+    assert max_abs(be.copy_m(), sim.m) <= 1e-10
+
+
+def test_dp45_fp64_matches_oracle():
+    nx, ny, nz = 32, 32, 2
+    mask = _disk_mask(nx, ny, nz, 30e-9, 8e-9, 2e-9)
+    adaptive = (1e-5, 1e-18, 1e-10, 0.8)
+    be, sim, _ = make_pair((nx, ny, nz), (2e-9, 2e-9, 2e-9), alpha=0.1, h_ext=(0, 30e-3 / MU0, 0),
+                           mask=mask, integrator=nf.DP45, adaptive=adaptive, seed=44)
+    dt = 1e-13
+    for _ in range(15):
+        st = be.step(dt)
+        r = sim.step(dt)
+        assert rel(st["dt_seconds"], r["dt_used"]) <= 1e-9
+        assert rel(st["suggested_next_dt"], r["suggested_next_dt"]) <= 1e-6
+        dt = st["suggested_next_dt"]
+    assert max_abs(be.copy_m(), sim.m) <= 1e-10
+    assert abs(st["time_seconds"] - sim.time) <= 1e-9 * sim.time
+    _energy_close(st, r, 1e-9)
+
+
+def test_fp32_mixed_vs_fp64_oracle():
+    kw = c1_kwargs()
+    be, sim, _ = make_pair(**kw, precision=nf.PRECISION_SINGLE)
+    for _ in range(100):
+        st = be.step(1e-13)
+        r = sim.step(1e-13)
+    dm = max_abs(be.copy_m(), sim.m)
+    print(f"C1 FP32-mixed vs FP64 oracle after 100 steps: {dm:.3e}")
+    assert dm <= 1e-5
+    assert rel(st["total_energy_joules"], r["e_total"]) <= 1e-4
+
+
+def test_fp32_mixed_3d_vs_fp64_oracle():
+    cells = (16, 16, 4)
+    be, sim, _ = make_pair(cells, (2e-9, 2e-9, 2e-9), alpha=0.5, h_ext=(10e-3 / MU0, 0, 0),
+                           precision=nf.PRECISION_SINGLE, seed=43)
+    for _ in range(100):
+        st = be.step(5e-14)
+        r = sim.step(5e-14)
+    dm = max_abs(be.copy_m(), sim.m)
+    print(f"3-D FP32-mixed vs FP64 oracle after 100 steps: {dm:.3e}")
+    assert dm <= 1e-5
+    assert rel(st["total_energy_joules"], r["e_total"]) <= 1e-4
+
+
+def test_newell_computed_in_library_matches_supplied_spectra():
+    for cells, thin in (((20, 12, 1), True), ((10, 8, 3), False)):
+        a, sim, _ = make_pair(cells, (2e-9, 3e-9, 2.5e-9), thin=thin, spectra="oracle")
+        b, _, _ = make_pair(cells, (2e-9, 3e-9, 2.5e-9), thin=thin, spectra="newell")
+        h = sim.observe()["h_demag"]
+        scale = np.abs(h).max()
+        assert max_abs(a.copy_field(nf.OBS_H_DEMAG), h) <= 1e-12 * scale
+        assert max_abs(b.copy_field(nf.OBS_H_DEMAG), h) <= 1e-12 * scale
+
+
+def test_projection_fallback_without_spectra():
+    nx, ny, nz = 6, 5, 2
+    d = (2e-9, 2e-9, 3e-9)
+    be, _, m0 = make_pair((nx, ny, nz), d, spectra=None, exchange=False)
+    # numpy restatement of demag_fp64.cu:102-148 on the (2nx, 2ny, 2nz) grid
+    px, py, pz = 2 * nx, 2 * ny, 2 * nz
+    M = np.zeros((3, pz, py, px))
+    M[:, :nz, :ny, :nx] = (8e5 * m0.reshape(nz, ny, nx, 3)).transpose(3, 0, 1, 2)
+    F = np.fft.fftn(M, axes=(1, 2, 3))
+    fi = lambda n: np.where(np.arange(n) <= n // 2, np.arange(n), np.arange(n) - n)
+    kx = 2 * np.pi * fi(px) / (px * d[0])
+    ky = 2 * np.pi * fi(py) / (py * d[1])
+    kz = 2 * np.pi * fi(pz) / (pz * d[2])
+    KZ, KY, KX = np.meshgrid(kz, ky, kx, indexing="ij")
+    k2 = KX ** 2 + KY ** 2 + KZ ** 2
+    k2[0, 0, 0] = 1.0
+    kdm = KX * F[0] + KY * F[1] + KZ * F[2]
+    H = np.stack([-KX * kdm / k2, -KY * kdm / k2, -KZ * kdm / k2])
+    H[:, 0, 0, 0] = 0
+    h = np.fft.ifftn(H, axes=(1, 2, 3)).real[:, :nz, :ny, :nx]
+    ref = h.transpose(1, 2, 3, 0).reshape(-1)
+    assert max_abs(be.copy_field(nf.OBS_H_DEMAG), ref) <= 1e-11 * np.abs(ref).max()
+
+
+def test_ms_map_and_time_dependent_field():
+    nx, ny = 24, 20
+    rng = np.random.default_rng(46)
+    ms_map = rng.uniform(6e5, 1e6, nx * ny)
+    ms_map[:7] = 0.0  # a few inactive cells
+    be, sim, _ = make_pair((nx, ny, 1), (4e-9, 4e-9, 3e-9), alpha=0.05,
+                           h_ext=(0, 0, 5e-3 / MU0), ac_field=(20e-3 / MU0, 0, 0), ac_freq=5e9,
+                           ms_map=ms_map, seed=46)
+    for _ in range(100):
+        st = be.step(1e-13)
+        r = sim.step(1e-13)
+    assert max_abs(be.copy_m(), sim.m) <= 1e-10
+    _energy_close(st, r, 1e-9)
+
+
+def test_transfers_previews_snapshots_uploads():
+    nx, ny, nz = 20, 12, 3
+    be, sim, _ = make_pair((nx, ny, nz), (2e-9, 2e-9, 2e-9), h_ext=(1e4, 0, 0), seed=3)
+    be.step(1e-14)
+    sim.step(1e-14)
+    m64 = be.copy_m()
+    m32 = be.copy_field(nf.OBS_M, dtype=np.float32)
+    assert np.array_equal(m32, m64.astype(np.float32))
+    # preview: box averages with the reference binning
+    prev = be.copy_preview(nf.OBS_M, (7, 5, 2), z_origin=1, z_stride=1)
+    grid = m64.reshape(nz, ny, nx, 3)
+    ref = np.zeros((2, 5, 7, 3))
+    for iz in range(2):
+        zs = min(1 + iz, nz - 1)
+        ze = min(max(1 + iz + 1, zs + 1), nz)
+        for iy in range(5):
+            y0, y1 = iy * ny // 5, max((iy + 1) * ny // 5, iy * ny // 5 + 1)
+            for ix in range(7):
+                x0, x1 = ix * nx // 7, max((ix + 1) * nx // 7, ix * nx // 7 + 1)
+                ref[iz, iy, ix] = grid[zs:ze, y0:y1, x0:x1].reshape(-1, 3).mean(axis=0)
+    assert max_abs(prev, ref.reshape(-1)) <= 1e-15
+    full = be.copy_preview(nf.OBS_M, (nx, ny, nz))
+    assert np.array_equal(full, m64)
+    # snapshot: SoA payload
+    snap = be.snapshot(nf.OBS_M)
+    assert np.array_equal(snap, m64.reshape(-1, 3).T)
+    hx = be.snapshot(nf.OBS_H_EXT)
+    assert np.all(hx[0] == 1e4) and np.all(hx[1:] == 0)
+    # upload + refresh recomputes the fields of the uploaded state
+    m_new = O.random_unit_vectors(99, nx * ny * nz)
+    be.upload_m(m_new)
+    be.refresh_observables()
+    sim.set_m(m_new)
+    obs = sim.observe()
+    assert max_abs(be.copy_m(), m_new) == 0.0
+    assert max_abs(be.copy_field(nf.OBS_H_EFF), obs["h_eff"]) <= 1e-12 * np.abs(obs["h_eff"]).max()
+    # stepping after an upload starts from the uploaded state
+    st = be.step(1e-14)
+    r = sim.step(1e-14)
+    assert max_abs(be.copy_m(), sim.m) <= 1e-12
+
+
+def test_step_n_equals_repeated_steps_and_is_deterministic():
+    kw = dict(cells=(32, 16, 2), cell_size=(2e-9, 2e-9, 2e-9), alpha=0.1, h_ext=(1e4, 2e4, 0))
+    a, _, _ = make_pair(**kw)
+    b, _, _ = make_pair(**kw)
+    for _ in range(25):
+        sa = a.step(3e-14)
+    sb = b.step_n(3e-14, 25)
+    assert np.array_equal(a.copy_m(), b.copy_m())
+    for k in ("exchange_energy_joules", "demag_energy_joules", "max_rhs_amplitude", "step"):
+        assert sa[k] == sb[k]
+
+
+def test_runtime_errors_are_reported():
+    be, _, _ = make_pair((8, 4, 2), (2e-9, 2e-9, 2e-9), demag=False)
+    with pytest.raises(nf.RunError, match="dt must be positive"):
+        be.step(0.0)
+    lib = nf.load_library()
+    out = np.zeros(5)
+    rc = lib.fullmag_fdm_backend_copy_field_f64(be.handle, nf.OBS_M, out.ctypes.data_as(nf._dp), 5)
+    assert rc == nf.ERR_INVALID
+    assert lib.fullmag_fdm_backend_last_error(be.handle) == b"out_len mismatch"
