@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark: Heun cell-updates/s of the FP32-mixed path vs the plain FP64 path.
+
+Workload (default, N = 1): 512 x 512 x 8 film of 2 nm cells, Ms = 8e5 A/m,
+A = 1.3e-11 J/m, alpha = 0.5, B = (10, 0, 0) mT, seeded random unit m
+(seed 43, the planner's generator), Heun dt = 5e-14 s; exchange + demag +
+Zeeman.  One "step" is one Heun step of the whole grid (2 097 152 cells).
+
+Reported (one JSON line on rank 0):
+  value   FP32-mixed cell-updates/s, whole job, state resident in HBM, timed
+          with CUDA events on the library's stream (max over ranks);
+  e2e     the same through the C ABI from host buffers: upload of m0 from
+          pinned memory, K fullmag_fdm_backend_step calls (stats read back
+          every step) and the final copy of m to host, all inside the timed
+          region;
+  fp64    the plain FP64 path's cell-updates/s and the FP32/FP64 ratio;
+  max_dm  max|m_fp32 - m_fp64| after the same K steps from the same m0;
+  roofline  the dominant kernel's algorithmic bytes per launch / its mean
+          launch time (CUDA events) against the measured HBM copy bandwidth;
+  cpu_baseline  the FP64 CPU port of the reference engine (oracle/) timed on
+          this host on one Heun step of the same grid.
+Multi-GPU: independent replicas (the FFT convolution is global and the
+workload does not shard), weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MU0 = 4.0 * np.pi * 1e-7
+WORKLOAD = dict(cells=(512, 512, 8), cell_size=(2e-9, 2e-9, 2e-9), ms=8.0e5, aex=1.3e-11,
+                alpha=0.5, gamma=2.211e5, b_mT=(10.0, 0.0, 0.0), seed=43, dt=5e-14)
+METRIC = "cell-updates/s FP32-mixed vs plain FP64, 1 B200, at max|dm|<=1e-5; HBM GB/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        time.sleep(0.25)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------- roofline model
+def kernel_bytes(name: str, g: dict, s: int) -> float:
+    """Algorithmic bytes of one launch of a library kernel (reads + writes of the
+    arrays it must touch once), for the 3-D demag path of grid g."""
+    nx, ny, nz = g["cells"]
+    n = nx * ny * nz
+    nkx, Ly = nx + 1, 2 * ny
+    cs = 2 * s
+    s1 = 3 * nz * nkx * ny * cs
+    s2 = 3 * nz * nkx * Ly * cs
+    octant = 6 * (nz + 1) * nkx * (ny + 1) * s
+    table = {
+        "demag_x_fwd": 3 * n * s + s1,
+        "demag_y_fwd": s1 + s2,
+        "demag_z_conv": 2 * s2 + octant,
+        "demag_y_inv": s2 + s1,
+        "demag_x_inv": s1 + 3 * n * s,
+        "stage_combine": 9 * n * s,
+        "stage_heun_corr": 15 * n * s,
+        "stage_eval": 9 * n * s,
+        "reduce_finalize": 0,
+    }
+    return float(table.get(name, 0))
+
+
+# --------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+
+    rank, world, local = env_rank()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(local)
+
+    from fullmag_b200 import native_fdm as nf
+
+    W = WORKLOAD
+    nx, ny, nz = W["cells"]
+    n = nx * ny * nz
+    K, warm = args.steps, max(3, args.warmup)
+    dt = W["dt"]
+    m0 = nf.random_unit_vectors(W["seed"], n)
+    m0_pinned = torch.from_numpy(m0).pin_memory()
+    h = tuple(b * 1e-3 / MU0 for b in W["b_mT"])
+
+    def make(prec):
+        plan = nf.FdmPlan(cells=W["cells"], cell_size=W["cell_size"], initial_magnetization=m0,
+                          saturation_magnetisation=W["ms"], exchange_stiffness=W["aex"],
+                          damping=W["alpha"], gyromagnetic_ratio=W["gamma"], precision=prec,
+                          external_field=h, demag_source=nf.DEMAG_NEWELL)
+        return nf.NativeFdmBackend(plan)
+
+    def barrier_sync():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    sampler_out = None
+    for prec, tag in ((nf.PRECISION_DOUBLE, "fp64"), (nf.PRECISION_SINGLE, "fp32")):
+        be = make(prec)
+        stream = torch.cuda.ExternalStream(be.stream())
+        be.step_n(dt, warm)
+        # device-resident timing
+        barrier_sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(local) if tag == "fp32" else None
+        if sampler:
+            sampler.__enter__()
+        e0.record(stream)
+        be.step_n(dt, K)
+        e1.record(stream)
+        e1.synchronize()
+        if sampler:
+            sampler.__exit__(None, None, None)
+            sampler_out = sampler.summary()
+        barrier_sync()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        # per-kernel device time (CUDA events around every launch, same stream)
+        be.set_profiling(True)
+        be.profile_reset()
+        be.step_n(dt, K)
+        prof = be.profile()
+        be.set_profiling(False)
+        # end to end through the C ABI from host buffers
+        barrier_sync()
+        m_host = np.empty(3 * n)
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        be.upload_m(m0_pinned.numpy())
+        for _ in range(K):
+            be.step(dt)
+        m_host[:] = be.copy_m()
+        f1.record(stream)
+        f1.synchronize()
+        barrier_sync()
+        ms_e2e = max_over_ranks(f0.elapsed_time(f1))
+        results[tag] = dict(ms=ms, prof=prof, ms_e2e=ms_e2e, m=m_host,
+                            mem=be.memory_info()[0])
+        be.close()
+
+    s32 = 4
+    cells_job = n * K * world
+    v32 = cells_job / (results["fp32"]["ms"] * 1e-3)
+    v64 = cells_job / (results["fp64"]["ms"] * 1e-3)
+    e2e32 = cells_job / (results["fp32"]["ms_e2e"] * 1e-3)
+    max_dm = float(np.abs(results["fp32"]["m"] - results["fp64"]["m"]).max())
+
+    peak, peak_kind = hbm_peak()
+    prof = results["fp32"]["prof"]
+    dom = max((k for k in prof if k != "reduce_finalize"), key=lambda k: prof[k][0])
+    dom_ms, dom_launch = prof[dom]
+    dom_bytes = kernel_bytes(dom, W, s32)
+    achieved = dom_bytes / (dom_ms * 1e-3 / dom_launch) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("fp32", {}).get(dom)
+        except Exception:
+            traffic = None
+    launches = int(sum(c for _, c in prof.values()) // 1)
+    step_bytes = sum(kernel_bytes(k, W, s32) * c for k, (_, c) in prof.items()) / K
+    kernels = {k: {"ms_per_launch": round(v[0] / v[1], 5), "launches_per_step": v[1] / K,
+                   "gbs": round(kernel_bytes(k, W, s32) / (v[0] * 1e-3 / v[1]) / 1e9, 1)}
+               for k, v in sorted(prof.items())}
+    prof64 = results["fp64"]["prof"]
+    kernels64 = {k: {"ms_per_launch": round(v[0] / v[1], 5),
+                     "gbs": round(kernel_bytes(k, W, 8) / (v[0] * 1e-3 / v[1]) / 1e9, 1)}
+                 for k, v in sorted(prof64.items())}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample()
+
+    if rank == 0:
+        bi = 3 * n * 8 / K
+        bo = (96 + 3 * n * 8 / K)
+        line = {
+            "metric": METRIC, "value": v32, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": K, "warmup": warm, "ms_per_step": results["fp32"]["ms"] / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32-mixed (f64 Newell setup, renormalisation, energies)",
+            "data": "synthetic (seeded random unit m, the reference planner's generator)",
+            "config": {"workload": "512x512x8 film, 2 nm cells, Heun dt=5e-14 s, exchange+demag+Zeeman",
+                       "cells": n, "padded_fft": [1024, 1024, 16], "parallelism": f"replicas x{world}",
+                       "l2": "working set > 126 MB L2 per step (no flush needed)"},
+            "fp64": {"value": v64, "ms_per_step": results["fp64"]["ms"] / K,
+                     "speedup_fp32_over_fp64": v32 / v64, "kernels": kernels64},
+            "max_dm_fp32_vs_fp64": max_dm,
+            "e2e": {"value": e2e32, "unit": "cell-updates/s", "h2d_bytes_per_step": bi,
+                    "d2h_bytes_per_step": bo,
+                    "fp64_value": cells_job / (results["fp64"]["ms_e2e"] * 1e-3)},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
+                         "algorithmic_bytes_per_launch": dom_bytes, "traffic": traffic},
+            "step_roofline": {"algorithmic_bytes_per_step": step_bytes,
+                              "achieved_gbs": step_bytes / (results["fp32"]["ms"] / K * 1e-3) / 1e9},
+            "kernels": kernels,
+            "gpu_launches": launches,
+            "device_bytes": results["fp32"]["mem"],
+            "clocks": sampler_out,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------- CPU (oracle) legs
+def _oracle_problem(nx, ny, nz):
+    from oracle import oracle as O
+    W = WORKLOAD
+    h = tuple(b * 1e-3 / MU0 for b in W["b_mT"])
+    return O, O.Problem(nx, ny, nz, *W["cell_size"], ms=W["ms"], aex=W["aex"], alpha=W["alpha"],
+                        gamma=W["gamma"], h_ext=h)
+
+
+def cpu_baseline_sample():
+    """One Heun step of the full grid on the FP64 CPU port (about 10-30 s)."""
+    O, p = _oracle_problem(*WORKLOAD["cells"])
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    nx, ny, nz = WORKLOAD["cells"]
+    sim = O.Simulation(p, O.random_unit_vectors(WORKLOAD["seed"], nx * ny * nz))
+    t0 = time.perf_counter()
+    sim.step(WORKLOAD["dt"])
+    el = time.perf_counter() - t0
+    return {"value": nx * ny * nz / el, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+            "sample": f"1 Heun step of the full {nx}x{ny}x{nz} grid, FP64, OpenMP pointwise loops, "
+                      f"serial FFT lines as in the reference ({el:.1f} s)"}
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    O = None
+    threads = os.cpu_count() or 1
+    # bounded sample per step: the largest film of the workload's shape whose
+    # W + K steps fit in about three minutes of this host's CPU time
+    nx, ny, nz = WORKLOAD["cells"]
+    O, p = _oracle_problem(64, 64, nz)
+    O.set_threads(threads)
+    sim = O.Simulation(p, O.random_unit_vectors(WORKLOAD["seed"], 64 * 64 * nz))
+    t0 = time.perf_counter()
+    sim.step(WORKLOAD["dt"])
+    per_cell = (time.perf_counter() - t0) / (64 * 64 * nz)
+    budget = 180.0 / (args.steps + max(3, args.warmup))
+    side = 64
+    while side * 2 <= nx and per_cell * 1.3 * (2 * side) ** 2 * nz <= budget:
+        side *= 2
+    O, p = _oracle_problem(side, side, nz)
+    sim = O.Simulation(p, O.random_unit_vectors(WORKLOAD["seed"], side * side * nz))
+    for _ in range(max(3, args.warmup)):
+        sim.step(WORKLOAD["dt"])
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step(WORKLOAD["dt"])
+    el = time.perf_counter() - t0
+    v = side * side * nz * args.steps / el
+    sample = (f"{side}x{side}x{nz} film with the workload's physics (the full 512x512x8 grid "
+              f"takes ~{per_cell * 1.3 * nx * ny * nz:.0f} s per step here); FP64 CPU port of the "
+              f"reference engine, OpenMP pointwise loops, serial FFT lines")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random unit m)",
+            "config": {"workload": "512x512x8 film, 2 nm cells, Heun dt=5e-14 s, exchange+demag+Zeeman",
+                       "sample_grid": [side, side, nz], "parallelism": "host CPU"},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

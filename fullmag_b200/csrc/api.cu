@@ -140,7 +140,11 @@ bool extract_octant(Backend &b, const fullmag_fdm_plan_desc *plan, int Lzs,
 }
 
 // k k^T / k^2 on the padded grid, the reference's fallback without spectra
-// (native/backends/fdm/src/demag_fp64.cu:102-148).
+// (native/backends/fdm/src/demag_fp64.cu:102-148).  The reference uses +k at
+// Nyquist indices, so its tensor is not Hermitian there, and it keeps the real
+// part of the inverse transform: that equals convolving with the Hermitian
+// part of the tensor, whose off-diagonal term vanishes wherever exactly one of
+// its two axes sits at a Nyquist index.  The octant below stores that part.
 void projection_octant(Backend &b, std::vector<double> (&spec)[6]) {
     const int KX = b.nkx, KY = b.KY, KZ = b.KZ;
     for (auto &s : spec) s.assign((size_t)KZ * KX * KY, 0.0);
@@ -156,9 +160,10 @@ void projection_octant(Backend &b, std::vector<double> (&spec)[6]) {
                 spec[0][o] = qx * qx / q2;
                 spec[1][o] = qy * qy / q2;
                 spec[2][o] = qz * qz / q2;
-                spec[3][o] = qx * qy / q2;
-                spec[4][o] = qx * qz / q2;
-                spec[5][o] = qy * qz / q2;
+                const bool nyx = 2 * kx == b.Lx, nyy = 2 * ky == b.Ly, nyz = 2 * kz == b.Lz;
+                spec[3][o] = (nyx != nyy) ? 0.0 : qx * qy / q2;
+                spec[4][o] = (nyx != nyz) ? 0.0 : qx * qz / q2;
+                spec[5][o] = (nyy != nyz) ? 0.0 : qy * qz / q2;
             }
 }
 
@@ -550,6 +555,35 @@ int fullmag_fdm_backend_memory_info(fullmag_fdm_backend *h, uint64_t *bytes, uin
     if (bytes) *bytes = h->b.arena_bytes;
     if (dims) { dims[0] = h->b.Lx; dims[1] = h->b.Ly; dims[2] = h->b.Lz; }
     return FULLMAG_FDM_OK;
+}
+
+int fullmag_fdm_backend_get_stream(fullmag_fdm_backend *h, void **out) {
+    if (!h || !out) return FULLMAG_FDM_ERR_INVALID;
+    *out = (void *)h->b.stream;
+    return h->b.stream ? FULLMAG_FDM_OK : FULLMAG_FDM_ERR_INVALID;
+}
+
+void fullmag_fdm_random_unit_vectors(uint64_t seed, uint64_t count, double *out) {
+    if (!out) return;
+    uint64_t state = seed;
+    for (uint64_t v = 0; v < count; ++v) {
+        double c[3];
+        for (;;) {
+            for (int i = 0; i < 3; ++i) {
+                state ^= state << 13;
+                state ^= state >> 7;
+                state ^= state << 17;
+                c[i] = ((double)state / (double)UINT64_MAX) * 2.0 - 1.0;
+            }
+            const double nrm = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+            if (nrm > 1e-10) {
+                out[3 * v] = c[0] / nrm;
+                out[3 * v + 1] = c[1] / nrm;
+                out[3 * v + 2] = c[2] / nrm;
+                break;
+            }
+        }
+    }
 }
 
 int fullmag_fdm_newell_spectra(uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz,

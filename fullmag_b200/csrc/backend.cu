@@ -300,7 +300,7 @@ struct Impl {
         if (!demag(b, b.mstage, b.hd)) return false;
         // corrector at m_p: k2 and m <- normalize(m0 + (k1 + k2) dt/2)
         StageArgs<T> s = stage_args(b, b.mstage, b.time + dt);
-        s.kout = (T *)b.k[1];
+        s.kout = nullptr;  // k2 is consumed in registers
         s.m0 = (T *)b.m;
         s.k1 = (const T *)b.k[0];
         s.half_dt = 0.5 * dt;

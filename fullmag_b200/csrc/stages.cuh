@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
         double ms_i;
         const bool act = st_active(a, i, ms_i);
         if (!act) {
-            a.kout[i] = T(0); a.kout[n + i] = T(0); a.kout[2 * n + i] = T(0);
+            if (a.kout) { a.kout[i] = T(0); a.kout[n + i] = T(0); a.kout[2 * n + i] = T(0); }
             if (a.hex_out) { a.hex_out[i] = T(0); a.hex_out[n + i] = T(0); a.hex_out[2 * n + i] = T(0); }
             if (a.heff_out) { a.heff_out[i] = T(0); a.heff_out[n + i] = T(0); a.heff_out[2 * n + i] = T(0); }
             if (MODE == MODE_HEUN_CORR) {
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
         const T pr = a.precession ? T(1) : T(0);
         const T r0 = (pr * p0 + q0 * al) * gb, r1 = (pr * p1 + q1 * al) * gb,
                 r2 = (pr * p2 + q2 * al) * gb;
-        a.kout[i] = r0; a.kout[n + i] = r1; a.kout[2 * n + i] = r2;
+        if (a.kout) { a.kout[i] = r0; a.kout[n + i] = r1; a.kout[2 * n + i] = r2; }
         if (a.hex_out) { a.hex_out[i] = h0; a.hex_out[n + i] = h1; a.hex_out[2 * n + i] = h2; }
         if (a.heff_out) { a.heff_out[i] = e0; a.heff_out[n + i] = e1; a.heff_out[2 * n + i] = e2; }
 
@@ -241,9 +241,9 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
                     acc[Q_EEX] += coeff * (dx_ * dx_ + dy_ * dy_ + dz_ * dz_) * a.dinv[q];
                 }
             }
-            const double cmul_ = ms_i * a.vol * kMu0;
-            acc[Q_EDEMAG] += -0.5 * cmul_ * (m0d * (double)d0 + m1d * (double)d1 + m2d * (double)d2);
-            acc[Q_EEXT] += -cmul_ * (m0d * (double)hex0 + m1d * (double)hex1 + m2d * (double)hex2);
+            const double coef = ms_i * a.vol * kMu0;
+            acc[Q_EDEMAG] += -0.5 * coef * (m0d * (double)d0 + m1d * (double)d1 + m2d * (double)d2);
+            acc[Q_EEXT] += -coef * (m0d * (double)hex0 + m1d * (double)hex1 + m2d * (double)hex2);
             const double E0 = e0, E1 = e1, E2 = e2;
             acc[Q_HEFF2] = fmax(acc[Q_HEFF2], E0 * E0 + E1 * E1 + E2 * E2);
             const double D0 = d0, D1 = d1, D2 = d2;

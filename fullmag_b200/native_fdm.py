@@ -122,6 +122,7 @@ EXT_FUNCTIONS = (
     "fullmag_fdm_backend_set_profiling", "fullmag_fdm_backend_profile_count",
     "fullmag_fdm_backend_profile_entry", "fullmag_fdm_backend_profile_reset",
     "fullmag_fdm_backend_memory_info", "fullmag_fdm_newell_spectra",
+    "fullmag_fdm_backend_get_stream", "fullmag_fdm_random_unit_vectors",
 )
 
 _lib = None
@@ -174,6 +175,9 @@ def load_library(build_if_missing: bool = True):
     L.fullmag_fdm_backend_profile_reset.restype = None
     L.fullmag_fdm_backend_memory_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]
     L.fullmag_fdm_newell_spectra.argtypes = [C.c_uint32] * 3 + [C.c_double] * 3 + [C.c_int] + [_dp] * 6
+    L.fullmag_fdm_backend_get_stream.argtypes = [vp, C.POINTER(C.c_void_p)]
+    L.fullmag_fdm_random_unit_vectors.argtypes = [C.c_uint64, C.c_uint64, _dp]
+    L.fullmag_fdm_random_unit_vectors.restype = None
     _lib = L
     return L
 
@@ -184,6 +188,13 @@ def is_available() -> bool:
 
 class RunError(RuntimeError):
     pass
+
+
+def random_unit_vectors(seed: int, count: int) -> np.ndarray:
+    """Seeded m0 as the reference planner draws it (fullmag-plan/src/lib.rs:1928-1957)."""
+    out = np.zeros(3 * int(count))
+    load_library().fullmag_fdm_random_unit_vectors(int(seed), int(count), out.ctypes.data_as(_dp))
+    return out
 
 
 def newell_spectra(nx: int, ny: int, nz: int, dx: float, dy: float, dz: float,
@@ -437,6 +448,11 @@ class NativeFdmBackend:
 
     def profile_reset(self) -> None:
         self._lib.fullmag_fdm_backend_profile_reset(self._h)
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        self._check(self._lib.fullmag_fdm_backend_get_stream(self._h, C.byref(p)), "get_stream")
+        return int(p.value or 0)
 
     def memory_info(self) -> Tuple[int, Tuple[int, int, int]]:
         b = C.c_uint64()

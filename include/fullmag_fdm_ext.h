@@ -63,6 +63,15 @@ void fullmag_fdm_backend_profile_reset(fullmag_fdm_backend *handle);
 int fullmag_fdm_backend_memory_info(fullmag_fdm_backend *handle, uint64_t *out_device_bytes,
                                     uint32_t *out_fft_dims3);
 
+/* The CUDA stream the handle launches all its work on (a cudaStream_t), so
+ * callers can order their own work or record CUDA events around steps. */
+int fullmag_fdm_backend_get_stream(fullmag_fdm_backend *handle, void **out_stream);
+
+/* Seeded initial magnetisation as the reference planner draws it
+ * (crates/fullmag-plan/src/lib.rs:1928-1957): xorshift64 samples of the cube
+ * [-1, 1]^3, normalised; AoS f64 [3 * count]. */
+void fullmag_fdm_random_unit_vectors(uint64_t seed, uint64_t count, double *out_xyz);
+
 /* FP64 Newell spectra on the host, in the reference's interleaved complex
  * layout (length 2 * (2nx)(2ny)(2nz), or 2 * (2nx)(2ny) when thin_film_2d and
  * nz == 1): the same arrays the reference runner passes in the plan.

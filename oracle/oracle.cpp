@@ -116,8 +116,54 @@ struct FftPlan {
         }
     }
 
+    bool pow2() const { return n >= 2 && (n & (n - 1)) == 0; }
+
+    // Iterative Stockham autosort, radix 4 (one radix-2 pass when log2 n is odd),
+    // ping-pong between data and work; same twiddle table as the recursive path.
+    void execute_pow2(cplx *data, std::vector<cplx> &work) const {
+        work.resize(n);
+        cplx *a = data, *b = work.data();
+        for (size_t Ns = 1; Ns < n;) {
+            const size_t R = ((n / Ns) % 4 == 0) ? 4 : 2;
+            const size_t m = n / R;
+            const size_t tstep = n / (Ns * R);
+            for (size_t jb = 0; jb < m; jb += Ns) {
+                for (size_t k = 0; k < Ns; ++k) {
+                    const size_t j = jb + k;
+                    if (R == 4) {
+                        cplx v0 = a[j], v1 = a[j + m], v2 = a[j + 2 * m], v3 = a[j + 3 * m];
+                        if (k) {
+                            v1 *= tw[k * tstep];
+                            v2 *= tw[2 * k * tstep];
+                            v3 *= tw[3 * k * tstep];
+                        }
+                        const cplx s02 = v0 + v2, d02 = v0 - v2, s13 = v1 + v3, d13 = v1 - v3;
+                        // multiply d13 by -i (forward) or +i (inverse)
+                        const cplx rot = (sign < 0) ? cplx(d13.imag(), -d13.real())
+                                                    : cplx(-d13.imag(), d13.real());
+                        cplx *o = b + jb * 4 + k;
+                        o[0] = s02 + s13;
+                        o[Ns] = d02 + rot;
+                        o[2 * Ns] = s02 - s13;
+                        o[3 * Ns] = d02 - rot;
+                    } else {
+                        cplx v0 = a[j], v1 = a[j + m];
+                        if (k) v1 *= tw[k * tstep];
+                        cplx *o = b + jb * 2 + k;
+                        o[0] = v0 + v1;
+                        o[Ns] = v0 - v1;
+                    }
+                }
+            }
+            std::swap(a, b);
+            Ns *= R;
+        }
+        if (a != data) std::memcpy((void *)data, (const void *)a, n * sizeof(cplx));
+    }
+
     void execute(cplx *data, std::vector<cplx> &work) const {
         if (n <= 1) return;
+        if (pow2()) { execute_pow2(data, work); return; }
         work.resize(2 * n + 64);
         cplx *in = work.data();
         cplx *scratch = work.data() + n;
@@ -381,8 +427,35 @@ struct Problem {
             const double *s = sp.data() + 2 * plen * c;
             for (size_t i = 0; i < plen; ++i) dst[i] = cplx(s[2 * i], s[2 * i + 1]);
         };
+        if (d.symmetric_kernel) symmetrize(sp);
         take(0, kxx); take(1, kyy); take(2, kzz); take(3, kxy); take(4, kxz); take(5, kyz);
         for (auto *b : {&bmx, &bmy, &bmz, &bhx, &bhy, &bhz}) b->assign(plen, cplx(0, 0));
+    }
+
+    // Replace each interleaved spectrum by its exactly even/odd real part: the
+    // value at the octant (k <= L/2 per axis) mirrored with the component's parity.
+    void symmetrize(std::vector<double> &sp) const {
+        const int oddx[6] = {0, 0, 0, 1, 1, 0}, oddy[6] = {0, 0, 0, 1, 0, 1}, oddz[6] = {0, 0, 0, 0, 1, 1};
+        std::vector<double> re(plen);
+        for (int c = 0; c < 6; ++c) {
+            double *s = sp.data() + 2 * plen * c;
+            const bool imag2d = d.thin_film_2d && (oddx[c] != oddy[c]);
+            for (size_t i = 0; i < plen; ++i) re[i] = s[2 * i];
+            for (size_t kz = 0; kz < pz; ++kz)
+                for (size_t ky = 0; ky < py; ++ky)
+                    for (size_t kx = 0; kx < px; ++kx) {
+                        const size_t kxo = kx <= px / 2 ? kx : px - kx;
+                        const size_t kyo = ky <= py / 2 ? ky : py - ky;
+                        const size_t kzo = kz <= pz / 2 ? kz : pz - kz;
+                        double sg = 1.0;
+                        if (kx > px / 2 && oddx[c]) sg = -sg;
+                        if (ky > py / 2 && oddy[c]) sg = -sg;
+                        if (kz > pz / 2 && oddz[c]) sg = -sg;
+                        const size_t i = kx + px * (ky + py * kz);
+                        s[2 * i] = imag2d ? 0.0 : sg * re[kxo + px * (kyo + py * kzo)];
+                        s[2 * i + 1] = 0.0;
+                    }
+        }
     }
 
     // exchange_field_from_vectors (lib.rs:2247-2299) + region LUT (exchange_fp64.cu:80-114)
@@ -419,10 +492,15 @@ struct Problem {
                 }
                 double inv[3] = {1.0 / dx2, 1.0 / dy2, 1.0 / dz2};
                 double pref = 2.0 / (MU0 * ms_at(f));
+                // summation order of exchange_fp64.cu:102-112: xp, xm, yp, ym, zp, zm
+                const int order[6] = {1, 0, 3, 2, 5, 4};
                 V3 h;
                 for (int cc = 0; cc < 3; ++cc) {
                     double s = 0.0;
-                    for (int q = 0; q < 6; ++q) s += a[q] * (v[q][cc] - c[cc]) * inv[q / 2];
+                    for (int o = 0; o < 6; ++o) {
+                        const int q = order[o];
+                        s += a[q] * (v[q][cc] - c[cc]) * inv[q / 2];
+                    }
                     h[cc] = pref * s;
                 }
                 out[f] = h;

@@ -55,6 +55,10 @@ typedef struct {
     double h_ac[3];
     double ac_freq;
     int thin_film_2d;         /* demag through the 2-D (nz = 1) spectra, like the GPU runner path */
+    /* 1: convolve with the exactly even/odd part of the Newell spectra (real
+     * octant mirrored with parity; the form the CUDA library stores) instead of
+     * the reference's spectra, which carry rounding noise on the symmetry planes. */
+    int symmetric_kernel;
 } oracle_desc;
 
 typedef struct {

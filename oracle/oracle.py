@@ -36,7 +36,7 @@ class OracleDesc(C.Structure):
         ("max_error", C.c_double), ("dt_min", C.c_double), ("dt_max", C.c_double),
         ("headroom", C.c_double),
         ("h_ac", C.c_double * 3), ("ac_freq", C.c_double),
-        ("thin_film_2d", C.c_int),
+        ("thin_film_2d", C.c_int), ("symmetric_kernel", C.c_int),
     ]
 
 
@@ -162,6 +162,7 @@ class Problem:
     h_ac: Optional[Sequence[float]] = None
     ac_freq: float = 0.0
     thin_film_2d: bool = False
+    symmetric_kernel: bool = False
     _keep: list = field(default_factory=list, repr=False)
 
     def desc(self) -> OracleDesc:
@@ -199,6 +200,7 @@ class Problem:
         d.max_error, d.dt_min, d.dt_max, d.headroom = (
             self.max_error, self.dt_min, self.dt_max, self.headroom)
         d.thin_film_2d = int(self.thin_film_2d)
+        d.symmetric_kernel = int(self.symmetric_kernel)
         return d
 
 

@@ -17,8 +17,10 @@ def c1_kwargs():
 def make_pair(cells, cell_size, ms=8e5, aex=1.3e-11, alpha=0.02, gamma=2.211e5, h_ext=None,
               seed=42, m0=None, mask=None, regions=None, lut=None, demag=True, exchange=True,
               precision=nf.PRECISION_DOUBLE, integrator=nf.HEUN, thin=None, adaptive=None,
-              pure_damping=False, spectra="oracle", ms_map=None, ac_field=None, ac_freq=0.0):
-    """Returns (backend, oracle simulation, m0)."""
+              pure_damping=False, spectra="oracle", ms_map=None, ac_field=None, ac_freq=0.0,
+              symmetric_kernel=False):
+    """Returns (backend, oracle simulation, m0).  symmetric_kernel=True makes the
+    oracle convolve with the exactly even/odd Newell spectra the library stores."""
     nx, ny, nz = cells
     n = nx * ny * nz
     if m0 is None:
@@ -44,7 +46,7 @@ def make_pair(cells, cell_size, ms=8e5, aex=1.3e-11, alpha=0.02, gamma=2.211e5, 
                      precession=not pure_damping, exchange=exchange, demag=demag, h_ext=h_ext,
                      active_mask=mask, region_mask=regions, exchange_lut=lut,
                      ms_map=ms_map, h_ac=ac_field, ac_freq=ac_freq,
-                     thin_film_2d=thin and nz == 1)
+                     thin_film_2d=thin and nz == 1, symmetric_kernel=symmetric_kernel)
     if adaptive is not None:
         prob.max_error, prob.dt_min, prob.dt_max, prob.headroom = adaptive
     sim = O.Simulation(prob, m0)
