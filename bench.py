@@ -14,7 +14,7 @@ Reported (one JSON line on rank 0):
           every step) and the final copy of m to host, all inside the timed
           region;
   fp64    the plain FP64 path's cell-updates/s and the FP32/FP64 ratio;
-  max_dm  max|m_fp32 - m_fp64| after the same K steps from the same m0;
+  max_dm  max|m_fp32 - m_fp64| after the workload's 2000 steps from the same m0;
   roofline  the dominant kernel's algorithmic bytes per launch / its mean
           launch time (CUDA events) against the measured HBM copy bandwidth;
   cpu_baseline  the FP64 CPU port of the reference engine (oracle/) timed on
@@ -42,6 +42,7 @@ MU0 = 4.0 * np.pi * 1e-7
 WORKLOAD = dict(cells=(512, 512, 8), cell_size=(2e-9, 2e-9, 2e-9), ms=8.0e5, aex=1.3e-11,
                 alpha=0.5, gamma=2.211e5, b_mT=(10.0, 0.0, 0.0), seed=43, dt=5e-14)
 METRIC = "cell-updates/s FP32-mixed vs plain FP64, 1 B200, at max|dm|<=1e-5; HBM GB/s"
+ACCURACY_STEPS = 2000  # the workload's step count; max|dm| FP32-mixed vs FP64 is taken there
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -239,7 +240,11 @@ def run_ours(args):
         f1.synchronize()
         barrier_sync()
         ms_e2e = max_over_ranks(f0.elapsed_time(f1))
-        results[tag] = dict(ms=ms, prof=prof, ms_e2e=ms_e2e, m=m_host,
+        # accuracy run: the workload's full 2000 steps from m0
+        be.upload_m(m0)
+        be.step_n(dt, ACCURACY_STEPS)
+        m_acc = be.copy_m()
+        results[tag] = dict(ms=ms, prof=prof, ms_e2e=ms_e2e, m=m_acc,
                             mem=be.memory_info()[0])
         be.close()
 
@@ -291,7 +296,7 @@ def run_ours(args):
                        "l2": "working set > 126 MB L2 per step (no flush needed)"},
             "fp64": {"value": v64, "ms_per_step": results["fp64"]["ms"] / K,
                      "speedup_fp32_over_fp64": v32 / v64, "kernels": kernels64},
-            "max_dm_fp32_vs_fp64": max_dm,
+            "max_dm_fp32_vs_fp64": max_dm, "max_dm_after_steps": ACCURACY_STEPS,
             "e2e": {"value": e2e32, "unit": "cell-updates/s", "h2d_bytes_per_step": bi,
                     "d2h_bytes_per_step": bo,
                     "fp64_value": cells_job / (results["fp64"]["ms_e2e"] * 1e-3)},

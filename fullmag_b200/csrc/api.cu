@@ -242,6 +242,12 @@ bool create_impl(Backend &b, const fullmag_fdm_plan_desc *plan, const fullmag_fd
         demag_src = ext->demag_source;
     }
     if (!b.has_ms_map && !(b.ms > 0)) { b.last_error = "saturation_magnetisation must be positive"; return false; }
+    {
+        // FULLMAG_FDM_FFT=stockham keeps the shared-memory Stockham FFT even for
+        // power-of-two lengths (both FFT paths are covered by the parity tests)
+        const char *f = std::getenv("FULLMAG_FDM_FFT");
+        b.force_stockham = f && std::strcmp(f, "stockham") == 0;
+    }
     if (b.has_mask) b.mask_host.assign(plan->active_mask, plan->active_mask + b.n);
 
     // demag geometry

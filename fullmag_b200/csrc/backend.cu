@@ -16,14 +16,53 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "backend.hpp"
 #include "backend_impl.hpp"
 #include "demag.cuh"
+#include "demag_reg.cuh"
 #include "newell_host.hpp"
 #include "stages.cuh"
 
 namespace fm {
+
+// exp(-2 pi i k / 64), k < 64, for the register FFTs (per device).
+bool upload_tw64(Backend &b) {
+    double2 d[64];
+    float2 f[64];
+    for (int k = 0; k < 64; ++k) {
+        const double a = 2.0 * kPi * (double)k / 64.0;
+        d[k] = make_double2(std::cos(a), -std::sin(a));
+        f[k] = make_float2((float)d[k].x, (float)d[k].y);
+    }
+    return cuda_ok(b, cudaMemcpyToSymbol(c_tw64d, d, sizeof(d)), "twiddle64 d") &&
+           cuda_ok(b, cudaMemcpyToSymbol(c_tw64f, f, sizeof(f)), "twiddle64 f");
+}
+
+template <int V> using IC = std::integral_constant<int, V>;
+
+// (L1, L2) split of a power-of-two line length, as fftreg.cuh's l2_for.
+template <class F>
+static bool with_split(int L, F &&f) {
+    switch (L) {
+        case 2: f(IC<2>{}, IC<1>{}); return true;
+        case 4: f(IC<4>{}, IC<1>{}); return true;
+        case 8: f(IC<8>{}, IC<1>{}); return true;
+        case 16: f(IC<16>{}, IC<1>{}); return true;
+        case 32: f(IC<32>{}, IC<1>{}); return true;
+        case 64: f(IC<8>{}, IC<8>{}); return true;
+        case 128: f(IC<16>{}, IC<8>{}); return true;
+        case 256: f(IC<16>{}, IC<16>{}); return true;
+        case 512: f(IC<32>{}, IC<16>{}); return true;
+        case 1024: f(IC<32>{}, IC<32>{}); return true;
+        case 2048: f(IC<64>{}, IC<32>{}); return true;
+        case 4096: f(IC<64>{}, IC<64>{}); return true;
+        default: return false;
+    }
+}
+
+static bool is_pow2(int L) { return L >= 2 && (L & (L - 1)) == 0; }
 
 // ---------------------------------------------------------------------------
 // helpers
@@ -120,7 +159,135 @@ struct Impl {
         return a;
     }
 
+    // Register-FFT path: power-of-two lengths, x/y <= 1024 (FP64) or 4096
+    // (FP32), z <= 16 (FP64) or 32 (FP32) since a thread holds 3 z lines.
+    static bool configure_reg(Backend &b) {
+        const bool dbl = sizeof(T) == 8;
+        const int maxxy = dbl ? 1024 : 4096, maxz = dbl ? 16 : 32;
+        if (!is_pow2(b.Lx) || !is_pow2(b.Ly) || b.Lx > maxxy || b.Ly > maxxy) return false;
+        if (!b.thin && (!is_pow2(b.Lz) || b.Lz > maxz)) return false;
+        const size_t sz = sizeof(C), maxs = 200 * 1024;
+        const int target = (dbl && b.Lx >= 512) ? 128 : 256;
+        bool ok = true;
+        // x passes: lines_x complex lines (row pairs) of L2 threads
+        with_split(b.Lx, [&](auto l1, auto l2) {
+            constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
+            if constexpr (sizeof(T) == 8 && L1 > 32) { ok = false; } else {
+                constexpr int TE = line_region<L1, L2>();
+                const int unit = L2 >= 32 ? 1 : 32 / L2;    // lines per warp multiple
+                int lp = std::max(1, target / L2);
+                lp = std::min(lp, std::max(unit, ((b.ny + 1) / 2 + unit - 1) / unit * unit));
+                while (lp > unit && (size_t)(L1 * L2 + lp * TE) * sz > maxs) lp -= unit;
+                b.lines_x = lp;
+                b.thr_x = lp * L2;
+                b.rsm_x = (size_t)(L1 * L2 + lp * TE) * sz;
+                ok &= cuda_ok(b, cudaFuncSetAttribute(k_xf_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_x), "attr xf_r");
+                ok &= cuda_ok(b, cudaFuncSetAttribute(k_xi_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_x), "attr xi_r");
+            }
+        });
+        if (!ok) return false;
+        with_split(b.Ly, [&](auto l1, auto l2) {
+            constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
+            if constexpr (sizeof(T) == 8 && L1 > 32) { ok = false; } else {
+                if (b.thin) {
+                    constexpr int TE = line_region<L1, L2>();
+                    const int unit = L2 >= 32 ? 1 : 32 / L2;  // kb multiple so 3*kb*L2 % 32 == 0
+                    int kb = std::max(unit, (256 / (3 * L2)) / unit * unit);
+                    kb = std::min(kb, std::max(unit, (b.nkx + unit - 1) / unit * unit));
+                    while (kb > unit && (size_t)(L1 * L2 + 3 * kb * TE) * sz > maxs) kb -= unit;
+                    b.kb_y = kb;
+                    b.thr_yc = 3 * kb * L2;
+                    b.rsm_yc = (size_t)(L1 * L2 + 3 * kb * TE) * sz;
+                    ok &= b.rsm_yc <= 227 * 1024 && b.thr_yc <= 256;
+                    ok &= cuda_ok(b, cudaFuncSetAttribute(k_yc_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_yc), "attr yc_r");
+                } else {
+                    constexpr int TE = tile_elems(L1, L2);
+                    const int lpb = std::max(1, 256 / L2);
+                    b.lines_y = lpb;
+                    b.thr_y = lpb * L2;
+                    b.rsm_y = (size_t)(L1 * L2 + lpb * TE) * sz;
+                    ok &= cuda_ok(b, cudaFuncSetAttribute(k_yf_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_y), "attr yf_r");
+                    ok &= cuda_ok(b, cudaFuncSetAttribute(k_yi_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_y), "attr yi_r");
+                }
+            }
+        });
+        return ok;
+    }
+
+    static bool demag_reg(Backend &b, const void *m, void *hd) {
+        DemagArgs<T> a = demag_args(b, m, hd);
+        const int RB = 2 * b.lines_x;
+        dim3 gx((b.ny + RB - 1) / RB, b.nz, 3);
+        with_split(b.Lx, [&](auto l1, auto l2) {
+            constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
+            if constexpr (!(sizeof(T) == 8 && L1 > 32)) {
+                ProfScope p(b, "demag_x_fwd");
+                k_xf_r<T, L1, L2><<<gx, b.thr_x, b.rsm_x, b.stream>>>(a);
+            }
+        });
+        if (b.thin) {
+            with_split(b.Ly, [&](auto l1, auto l2) {
+                constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
+                if constexpr (!(sizeof(T) == 8 && L1 > 32)) {
+                    ProfScope p(b, "demag_y_conv");
+                    k_yc_r<T, L1, L2><<<(b.nkx + b.kb_y - 1) / b.kb_y, b.thr_yc, b.rsm_yc, b.stream>>>(a);
+                }
+            });
+        } else {
+            const long long lines = 3LL * b.nz * b.nkx;
+            const unsigned gy = (unsigned)((lines + b.lines_y - 1) / b.lines_y);
+            with_split(b.Ly, [&](auto l1, auto l2) {
+                constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
+                if constexpr (!(sizeof(T) == 8 && L1 > 32)) {
+                    ProfScope p(b, "demag_y_fwd");
+                    k_yf_r<T, L1, L2><<<gy, b.thr_y, b.rsm_y, b.stream>>>(a);
+                }
+            });
+            {
+                ProfScope p(b, "demag_z_conv");
+                const long long cols = (long long)b.nkx * b.Ly;
+                const unsigned gz = (unsigned)std::min<long long>((cols + 127) / 128, 148LL * 64);
+                // one thread per column up to 3 x 8 (FP64) / 3 x 16 (FP32) z points,
+                // a thread pair (split by kz parity) above
+                const bool dbl = sizeof(T) == 8;
+                const int P = (b.Lz > 8) ? 2 : 1;
+                const unsigned gz2 = (unsigned)std::min<long long>((cols * P + 127) / 128, 148LL * 64);
+                switch (b.Lz * 10 + P) {
+                    case 21: k_zc_r<T, 2, 1><<<gz2, 128, 0, b.stream>>>(a); break;
+                    case 41: k_zc_r<T, 4, 1><<<gz2, 128, 0, b.stream>>>(a); break;
+                    case 81: k_zc_r<T, 8, 1><<<gz2, 128, 0, b.stream>>>(a); break;
+                    case 162: k_zc_r<T, 16, 2><<<gz2, 128, 0, b.stream>>>(a); break;
+                    case 322: if constexpr (sizeof(T) == 4) k_zc_r<T, 32, 2><<<gz2, 128, 0, b.stream>>>(a); break;
+                    default: break;
+                }
+                (void)gz;
+            }
+            with_split(b.Ly, [&](auto l1, auto l2) {
+                constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
+                if constexpr (!(sizeof(T) == 8 && L1 > 32)) {
+                    ProfScope p(b, "demag_y_inv");
+                    k_yi_r<T, L1, L2><<<gy, b.thr_y, b.rsm_y, b.stream>>>(a);
+                }
+            });
+        }
+        with_split(b.Lx, [&](auto l1, auto l2) {
+            constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
+            if constexpr (!(sizeof(T) == 8 && L1 > 32)) {
+                ProfScope p(b, "demag_x_inv");
+                k_xi_r<T, L1, L2><<<gx, b.thr_x, b.rsm_x, b.stream>>>(a);
+            }
+        });
+        return check_launch(b, "demag (register FFT)");
+    }
+
     static bool configure(Backend &b) {
+        if (!upload_tw64(b)) return false;
+        if (!b.force_stockham && configure_reg(b)) {
+            b.use_reg = true;
+            return true;
+        }
+        b.use_reg = false;
+        if (!b.last_error.empty()) return false;
         const int budget = 100 * 1024;
         const int sz = (int)sizeof(C);
         auto lines_for = [&](int ld, int L, int per_line_mult, int maxl) {
@@ -162,6 +329,7 @@ struct Impl {
     // H_d(m) into hd.
     static bool demag(Backend &b, const void *m, void *hd) {
         if (!b.enable_demag) return true;
+        if (b.use_reg) return demag_reg(b, m, hd);
         DemagArgs<T> a = demag_args(b, m, hd);
         const int RB = 2 * b.lines_x;
         dim3 gx((b.ny + RB - 1) / RB, b.nz, 3);

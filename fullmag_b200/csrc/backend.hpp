@@ -63,6 +63,11 @@ struct Backend {
     void *s1 = nullptr, *s2 = nullptr, *spec = nullptr;
     int lines_x = 1, lines_y = 1, kt_z = 1, kb_y = 1;
     size_t smem_xf = 0, smem_yf = 0, smem_z = 0, smem_yc = 0;
+    // register-FFT path (power-of-two lengths): block sizes and shared memory
+    bool use_reg = false;
+    bool force_stockham = false;  // FULLMAG_FDM_FFT=stockham selects the shared-memory FFT
+    int thr_x = 0, thr_y = 0, thr_yc = 0;
+    size_t rsm_x = 0, rsm_y = 0, rsm_yc = 0;
 
     // ---- reductions ----
     int red_blocks = 0;

@@ -1,0 +1,295 @@
+// demag_reg.cuh — register-FFT versions of the five demag passes.
+//
+// Same data flow and buffers as demag.cuh (S1 [c][z][kx][y], S2 [c][z][kx][ky],
+// real octant spectra), but every line FFT is fft4step (fftreg.cuh): one
+// shared-memory round trip per line instead of one per radix-4 stage, no
+// integer division in the butterflies, compile-time twiddles inside each
+// thread.  Used whenever all padded lengths are powers of two within the
+// register limits; other lengths use demag.cuh.
+#pragma once
+
+#include "demag.cuh"
+#include "fftreg.cuh"
+
+namespace fm {
+
+template <int L1, int L2> __host__ __device__ constexpr int line_region() {
+    return tile_elems(L1, L2) > L1 * L2 ? tile_elems(L1, L2) : L1 * L2;
+}
+
+// ---------------------------------------------------------------------------
+// x forward: pack Ms*m (two rows per complex line), R2C, transposed store.
+// block = lines_x line groups of L2 threads; grid (ceil(ny / 2 lines_x), nz, 3)
+// ---------------------------------------------------------------------------
+template <typename T, int L1, int L2>
+__global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
+    using C = cx<T>;
+    constexpr int L = L1 * L2, TE = line_region<L1, L2>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw = reinterpret_cast<C *>(smem_raw);
+    C *region = tw + L;
+    const int LP = a.lines_x, RB = 2 * LP;
+    const int c = blockIdx.z, z = blockIdx.y, y0 = blockIdx.x * RB;
+    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twx[k];
+    __syncthreads();
+    const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;
+    const T *mc = a.m + (long long)c * a.n;
+    const int ya = y0 + 2 * q, yb = ya + 1, nx = a.nx, ny = a.ny;
+    const long long rowa = ((long long)z * ny + ya) * nx, rowb = rowa + nx;
+    C *line = region + q * TE;
+    auto in = [&](int j) -> C {
+        C v = mk<T>(0, 0);
+        if (j < nx) {
+            double msi;
+            if (ya < ny && cell_active(a, rowa + j, msi)) v.x = (T)((double)mc[rowa + j] * msi);
+            if (yb < ny && cell_active(a, rowb + j, msi)) v.y = (T)((double)mc[rowb + j] * msi);
+        }
+        return v;
+    };
+    auto out = [&](int k, C v) { line[k] = v; };
+    fft4step<L1, L2, false, false, true>(t, tw, line, in, out);
+    __syncthreads();
+    const int nkx = a.nkx;
+    for (int u = threadIdx.x; u < nkx * RB; u += blockDim.x) {
+        const int k = u / RB, r = u - k * RB, y = y0 + r;
+        if (y >= ny) continue;
+        const C *ln = region + (r >> 1) * TE;
+        const C zk = ln[k];
+        const C zm = ln[k == 0 ? 0 : L - k];
+        C o;
+        if ((r & 1) == 0) { o.x = T(0.5) * (zk.x + zm.x); o.y = T(0.5) * (zk.y - zm.y); }
+        else { o.x = T(0.5) * (zk.y + zm.y); o.y = T(-0.5) * (zk.x - zm.x); }
+        a.s1[(((long long)c * a.nz + z) * nkx + k) * ny + y] = o;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// x inverse: gather A/B half spectra (transposed), form Z = A + iB on the full
+// circle, C2R, crop, 1/P, mask.  Same grid as k_xf_r.
+// ---------------------------------------------------------------------------
+template <typename T, int L1, int L2>
+__global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
+    using C = cx<T>;
+    constexpr int L = L1 * L2, TE = line_region<L1, L2>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw = reinterpret_cast<C *>(smem_raw);
+    C *region = tw + L;
+    const int LP = a.lines_x, RB = 2 * LP, nx = a.nx, ny = a.ny, nkx = a.nkx;
+    const int c = blockIdx.z, z = blockIdx.y, y0 = blockIdx.x * RB;
+    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twx[k];
+    // Z[k] = A[k] + i B[k] (k <= nx), Z[L-k] = conj(A[k]) + i conj(B[k]); DC and
+    // Nyquist taken as real.  Row pairs (A, B) sit in adjacent lanes.
+    const int total = nkx * RB;
+    const int span = (total + 31) / 32 * 32;
+    for (int u = threadIdx.x; u < span; u += blockDim.x) {
+        const int k = u / RB, r = u - k * RB, y = y0 + r;
+        C v = mk<T>(0, 0);
+        if (u < total && y < ny) v = a.s1[(((long long)c * a.nz + z) * nkx + k) * ny + y];
+        const T bx = __shfl_down_sync(0xffffffffu, v.x, 1);
+        const T by = __shfl_down_sync(0xffffffffu, v.y, 1);
+        if (u < total && (r & 1) == 0) {
+            C A = v, B = mk<T>(bx, by);
+            C *ln = region + (r >> 1) * TE;
+            if (k == 0 || k == nx) {
+                ln[k] = mk<T>(A.x, B.x);
+            } else {
+                ln[k] = mk<T>(A.x - B.y, A.y + B.x);
+                ln[L - k] = mk<T>(A.x + B.y, -A.y + B.x);
+            }
+        }
+    }
+    __syncthreads();
+    const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;
+    const int ya = y0 + 2 * q, yb = ya + 1;
+    C *line = region + q * TE;
+    const T nrm = (T)a.norm;
+    T *hc = a.hd + (long long)c * a.n;
+    const long long rowa = ((long long)z * ny + ya) * nx, rowb = rowa + nx;
+    auto in = [&](int j) -> C { return line[j]; };
+    auto out = [&](int k, C v) {
+        if (k >= nx) return;
+        double msi;
+        if (ya < ny) hc[rowa + k] = cell_active(a, rowa + k, msi) ? v.x * nrm : T(0);
+        if (yb < ny) hc[rowb + k] = cell_active(a, rowb + k, msi) ? v.y * nrm : T(0);
+    };
+    fft4step<L1, L2, true, true, false>(t, tw, line, in, out);
+}
+
+// ---------------------------------------------------------------------------
+// y forward (3-D): S1 -> S2, line g = (c, z, kx); block = lines_y groups of L2
+// ---------------------------------------------------------------------------
+template <typename T, int L1, int L2>
+__global__ void __launch_bounds__(256) k_yf_r(DemagArgs<T> a) {
+    using C = cx<T>;
+    constexpr int L = L1 * L2, TE = tile_elems(L1, L2);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw = reinterpret_cast<C *>(smem_raw);
+    C *region = tw + L;
+    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twy[k];
+    __syncthreads();
+    const int q = threadIdx.x / L2, t = threadIdx.x - q * L2, ny = a.ny;
+    const long long total = 3LL * a.nz * a.nkx;
+    const long long g = (long long)blockIdx.x * a.lines_y + q;
+    const bool valid = g < total;
+    const C *src = a.s1 + g * ny;
+    C *dst = a.s2 + g * L;
+    auto in = [&](int j) -> C { return (valid && j < ny) ? src[j] : mk<T>(0, 0); };
+    auto out = [&](int k, C v) { if (valid) dst[k] = v; };
+    fft4step<L1, L2, false, false, false>(t, tw, region + q * TE, in, out);
+}
+
+// y inverse (3-D): S2 -> S1, keeps y < ny
+template <typename T, int L1, int L2>
+__global__ void __launch_bounds__(256) k_yi_r(DemagArgs<T> a) {
+    using C = cx<T>;
+    constexpr int L = L1 * L2, TE = tile_elems(L1, L2);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw = reinterpret_cast<C *>(smem_raw);
+    C *region = tw + L;
+    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twy[k];
+    __syncthreads();
+    const int q = threadIdx.x / L2, t = threadIdx.x - q * L2, ny = a.ny;
+    const long long total = 3LL * a.nz * a.nkx;
+    const long long g = (long long)blockIdx.x * a.lines_y + q;
+    const bool valid = g < total;
+    const C *src = a.s2 + g * L;
+    C *dst = a.s1 + g * ny;
+    auto in = [&](int j) -> C { return valid ? src[j] : mk<T>(0, 0); };
+    auto out = [&](int k, C v) { if (valid && k < ny) dst[k] = v; };
+    fft4step<L1, L2, true, false, false>(t, tw, region + q * TE, in, out);
+}
+
+// ---------------------------------------------------------------------------
+// z convolution (3-D): P threads per (kx, ky) column hold the three
+// components' z lines in registers: forward FFT, H = -N M per kz, inverse FFT,
+// keep z < nz.  With P = 2 the zero padding (x[z] = 0 for z >= nz = LZ/2) is
+// used to split the transform by the parity h of kz:
+//   X[2m + h] = FFT_nz(x[z] W_LZ^{h z})[m],
+//   x'[z]     = sum_h W_LZ^{-h z} IFFT_nz(X'_h)[z]        (z < nz),
+// so each thread of the pair holds 3 x nz values and the two halves are summed
+// with one shuffle exchange.
+// ---------------------------------------------------------------------------
+template <typename T, int LZ, int P>
+__global__ void __launch_bounds__(128) k_zc_r(DemagArgs<T> a) {
+    using C = cx<T>;
+    constexpr int NZL = LZ / P;  // points per thread
+    static_assert(P == 1 || P == 2, "z split");
+    const long long cols = (long long)a.nkx * a.Ly;
+    const int nz = a.nz, Ly = a.Ly, nkx = a.nkx;
+    const long long cs = (long long)nz * nkx * Ly;  // component stride in S2
+    const long long zs = (long long)nkx * Ly;
+    const int h = (P == 2) ? (threadIdx.x & 1) : 0;
+    const long long span = ((cols * P + 127) / 128) * 128;  // whole pairs and warps iterate together
+    for (long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x; tid < span;
+         tid += (long long)gridDim.x * blockDim.x) {
+        const long long col = tid / P;
+        const bool valid = col < cols;
+        const int kx = valid ? (int)(col / Ly) : 0;
+        const int ky = valid ? (int)(col - (long long)kx * Ly) : 0;
+        C *base = a.s2 + (long long)kx * Ly + ky;
+        C vx[NZL], vy[NZL], vz[NZL];
+#pragma unroll
+        for (int z = 0; z < NZL; ++z) {
+            const bool in = valid && z < nz;
+            vx[z] = in ? base[z * zs] : mk<T>(0, 0);
+            vy[z] = in ? base[cs + z * zs] : mk<T>(0, 0);
+            vz[z] = in ? base[2 * cs + z * zs] : mk<T>(0, 0);
+            if (P == 2 && h == 1 && z > 0) {
+                const C w = tw64<C>(z * (64 / LZ));  // W_LZ^z
+                vx[z] = cmul(vx[z], w); vy[z] = cmul(vy[z], w); vz[z] = cmul(vz[z], w);
+            }
+        }
+        fft_reg<NZL, false>(vx);
+        fft_reg<NZL, false>(vy);
+        fft_reg<NZL, false>(vz);
+        if (valid) {
+#pragma unroll
+            for (int p = 0; p < NZL; ++p) {
+                const int kz = P * brev<NZL>(p) + h;
+                tensor_apply(a, kx, ky, kz, vx[p], vy[p], vz[p]);
+            }
+        }
+        fft_reg_dit<NZL, true>(vx);
+        fft_reg_dit<NZL, true>(vy);
+        fft_reg_dit<NZL, true>(vz);
+        if constexpr (P == 1) {
+            if (valid) {
+#pragma unroll
+                for (int z = 0; z < NZL; ++z) {
+                    if (z < nz) {
+                        base[z * zs] = vx[z];
+                        base[cs + z * zs] = vy[z];
+                        base[2 * cs + z * zs] = vz[z];
+                    }
+                }
+            }
+        } else {
+            // thread h keeps z in [h nz/2, (h+1) nz/2); the partner's half arrives by shuffle
+#pragma unroll
+            for (int zz = 0; zz < NZL / 2; ++zz) {
+                // register selection by h without dynamic indexing
+                const int zlo = zz, zhi = zz + NZL / 2;
+                const int zmine = h ? zhi : zlo, zsend = h ? zlo : zhi;
+                C ox = h ? vx[zhi] : vx[zlo], oy = h ? vy[zhi] : vy[zlo], oz = h ? vz[zhi] : vz[zlo];
+                C sx = h ? vx[zlo] : vx[zhi], sy = h ? vy[zlo] : vy[zhi], sz = h ? vz[zlo] : vz[zhi];
+                if (h == 1) {
+                    // this thread's values carry W_LZ^{-z}
+                    const C w1 = tw64<C>(zhi * (64 / LZ));
+                    ox = cmulc(ox, w1); oy = cmulc(oy, w1); oz = cmulc(oz, w1);
+                    const C w2 = tw64<C>(zlo * (64 / LZ));
+                    sx = cmulc(sx, w2); sy = cmulc(sy, w2); sz = cmulc(sz, w2);
+                }
+                C rx, ry, rz;
+                rx.x = __shfl_xor_sync(0xffffffffu, sx.x, 1); rx.y = __shfl_xor_sync(0xffffffffu, sx.y, 1);
+                ry.x = __shfl_xor_sync(0xffffffffu, sy.x, 1); ry.y = __shfl_xor_sync(0xffffffffu, sy.y, 1);
+                rz.x = __shfl_xor_sync(0xffffffffu, sz.x, 1); rz.y = __shfl_xor_sync(0xffffffffu, sz.y, 1);
+                if (valid && zmine < nz) {
+                    base[zmine * zs] = cadd(ox, rx);
+                    base[cs + zmine * zs] = cadd(oy, ry);
+                    base[2 * cs + zmine * zs] = cadd(oz, rz);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// y convolution (2-D thin film): block = kb_y kx columns x 3 components, each
+// line a group of L2 threads: forward y, multiply with N(kx, ky, 0), inverse y.
+// ---------------------------------------------------------------------------
+template <typename T, int L1, int L2>
+__global__ void __launch_bounds__(256) k_yc_r(DemagArgs<T> a) {
+    using C = cx<T>;
+    constexpr int L = L1 * L2, TE = line_region<L1, L2>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw = reinterpret_cast<C *>(smem_raw);
+    C *region = tw + L;
+    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twy[k];
+    __syncthreads();
+    const int KB = a.kb_y, ny = a.ny, nkx = a.nkx;
+    const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;
+    const int comp = q / KB, kxl = q - comp * KB;
+    const int kx0 = blockIdx.x * KB, kx = kx0 + kxl;
+    const bool valid = kx < nkx;
+    C *line = region + q * TE;
+    C *g = a.s1 + ((long long)comp * nkx + kx) * ny;
+    auto in_g = [&](int j) -> C { return (valid && j < ny) ? g[j] : mk<T>(0, 0); };
+    auto out_s = [&](int k, C v) { line[k] = v; };
+    fft4step<L1, L2, false, false, true>(t, tw, line, in_g, out_s);
+    __syncthreads();
+    for (int u = threadIdx.x; u < KB * L; u += blockDim.x) {
+        const int kl = u / L, ky = u - kl * L;
+        if (kx0 + kl >= nkx) continue;
+        C *lx = region + (0 * KB + kl) * TE, *lyy = region + (1 * KB + kl) * TE,
+          *lz = region + (2 * KB + kl) * TE;
+        C mx = lx[ky], my = lyy[ky], mz = lz[ky];
+        tensor_apply(a, kx0 + kl, ky, 0, mx, my, mz);
+        lx[ky] = mx; lyy[ky] = my; lz[ky] = mz;
+    }
+    __syncthreads();
+    auto in_s = [&](int j) -> C { return line[j]; };
+    auto out_g = [&](int k, C v) { if (valid && k < ny) g[k] = v; };
+    fft4step<L1, L2, true, true, false>(t, tw, line, in_s, out_g);
+}
+
+}  // namespace fm

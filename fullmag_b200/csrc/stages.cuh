@@ -117,9 +117,9 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
     const T *mx = a.m, *my = a.m + n, *mz = a.m + 2 * n;
     const double s = a.t * a.ac_omega;
     const double sinv = (a.ac_omega != 0.0) ? sin(s) : 0.0;
-    const T hex0 = (T)(a.has_ext ? a.hext[0] + a.hac[0] * sinv : 0.0);
-    const T hex1 = (T)(a.has_ext ? a.hext[1] + a.hac[1] * sinv : 0.0);
-    const T hex2 = (T)(a.has_ext ? a.hext[2] + a.hac[2] * sinv : 0.0);
+    const double hx0 = a.has_ext ? a.hext[0] + a.hac[0] * sinv : 0.0;
+    const double hx1 = a.has_ext ? a.hext[1] + a.hac[1] * sinv : 0.0;
+    const double hx2 = a.has_ext ? a.hext[2] + a.hac[2] * sinv : 0.0;
 
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
@@ -138,8 +138,10 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
         const long long rem = i - (long long)z * sxy;
         const int y = (int)(rem / nx);
         const int x = (int)(rem - (long long)y * nx);
-        const T cx_ = mx[i], cy_ = my[i], cz_ = mz[i];
-        T h0 = T(0), h1 = T(0), h2 = T(0);  // exchange field
+        // arithmetic in FP64 from the stored values (FP64 or FP32)
+        using R = double;
+        const R cx_ = mx[i], cy_ = my[i], cz_ = mz[i];
+        R h0 = 0.0, h1 = 0.0, h2 = 0.0;  // exchange field
         long long nb[6];
         nb[0] = x < nx - 1 ? i + 1 : i;      // xp
         nb[1] = x > 0 ? i - 1 : i;           // xm
@@ -155,53 +157,54 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
             }
         }
         if (a.enable_exchange) {
+            const R ix2 = a.dinv[0], iy2 = a.dinv[1], iz2 = a.dinv[2];
             if (!a.region) {
-                const T pref = (T)(2.0 * a.aex / (kMu0 * ms_i));
-                T lx = (mx[nb[0]] - T(2) * cx_ + mx[nb[1]]) * a.idx2 +
-                       (mx[nb[2]] - T(2) * cx_ + mx[nb[3]]) * a.idy2 +
-                       (mx[nb[4]] - T(2) * cx_ + mx[nb[5]]) * a.idz2;
-                T ly = (my[nb[0]] - T(2) * cy_ + my[nb[1]]) * a.idx2 +
-                       (my[nb[2]] - T(2) * cy_ + my[nb[3]]) * a.idy2 +
-                       (my[nb[4]] - T(2) * cy_ + my[nb[5]]) * a.idz2;
-                T lz = (mz[nb[0]] - T(2) * cz_ + mz[nb[1]]) * a.idx2 +
-                       (mz[nb[2]] - T(2) * cz_ + mz[nb[3]]) * a.idy2 +
-                       (mz[nb[4]] - T(2) * cz_ + mz[nb[5]]) * a.idz2;
+                const R pref = 2.0 * a.aex / (kMu0 * ms_i);
+                const R lx = ((R)mx[nb[0]] - 2.0 * cx_ + (R)mx[nb[1]]) * ix2 +
+                             ((R)mx[nb[2]] - 2.0 * cx_ + (R)mx[nb[3]]) * iy2 +
+                             ((R)mx[nb[4]] - 2.0 * cx_ + (R)mx[nb[5]]) * iz2;
+                const R ly = ((R)my[nb[0]] - 2.0 * cy_ + (R)my[nb[1]]) * ix2 +
+                             ((R)my[nb[2]] - 2.0 * cy_ + (R)my[nb[3]]) * iy2 +
+                             ((R)my[nb[4]] - 2.0 * cy_ + (R)my[nb[5]]) * iz2;
+                const R lz = ((R)mz[nb[0]] - 2.0 * cz_ + (R)mz[nb[1]]) * ix2 +
+                             ((R)mz[nb[2]] - 2.0 * cz_ + (R)mz[nb[3]]) * iy2 +
+                             ((R)mz[nb[4]] - 2.0 * cz_ + (R)mz[nb[5]]) * iz2;
                 h0 = lx * pref; h1 = ly * pref; h2 = lz * pref;
             } else {
-                const T pref = (T)(2.0 / (kMu0 * ms_i));
+                const R pref = 2.0 / (kMu0 * ms_i);
                 const uint32_t rc = a.region[i];
-                const T inv[3] = {a.idx2, a.idy2, a.idz2};
-                T sx = T(0), sy = T(0), sz = T(0);
+                const R inv[3] = {ix2, iy2, iz2};
+                R sx = 0.0, sy = 0.0, sz = 0.0;
 #pragma unroll
                 for (int q = 0; q < 6; ++q) {
-                    const T aq = (T)a.lut[(size_t)rc * 256 + a.region[nb[q]]];
-                    sx += aq * (mx[nb[q]] - cx_) * inv[q >> 1];
-                    sy += aq * (my[nb[q]] - cy_) * inv[q >> 1];
-                    sz += aq * (mz[nb[q]] - cz_) * inv[q >> 1];
+                    const R aq = a.lut[(size_t)rc * 256 + a.region[nb[q]]];
+                    sx += aq * ((R)mx[nb[q]] - cx_) * inv[q >> 1];
+                    sy += aq * ((R)my[nb[q]] - cy_) * inv[q >> 1];
+                    sz += aq * ((R)mz[nb[q]] - cz_) * inv[q >> 1];
                 }
                 h0 = pref * sx; h1 = pref * sy; h2 = pref * sz;
             }
         }
-        T d0 = T(0), d1 = T(0), d2 = T(0);
+        R d0 = 0.0, d1 = 0.0, d2 = 0.0;
         if (a.enable_demag) { d0 = a.hd[i]; d1 = a.hd[n + i]; d2 = a.hd[2 * n + i]; }
-        const T e0 = (h0 + d0) + hex0, e1 = (h1 + d1) + hex1, e2 = (h2 + d2) + hex2;
+        const R e0 = (h0 + d0) + hx0, e1 = (h1 + d1) + hx1, e2 = (h2 + d2) + hx2;
         // Gilbert RHS: -gamma_bar (m x H + alpha m x (m x H))
-        const T p0 = cy_ * e2 - cz_ * e1, p1 = cz_ * e0 - cx_ * e2, p2 = cx_ * e1 - cy_ * e0;
-        const T q0 = cy_ * p2 - cz_ * p1, q1 = cz_ * p0 - cx_ * p2, q2 = cx_ * p1 - cy_ * p0;
-        const T al = (T)a.alpha, gb = (T)(-a.gamma_bar);
-        const T pr = a.precession ? T(1) : T(0);
-        const T r0 = (pr * p0 + q0 * al) * gb, r1 = (pr * p1 + q1 * al) * gb,
+        const R p0 = cy_ * e2 - cz_ * e1, p1 = cz_ * e0 - cx_ * e2, p2 = cx_ * e1 - cy_ * e0;
+        const R q0 = cy_ * p2 - cz_ * p1, q1 = cz_ * p0 - cx_ * p2, q2 = cx_ * p1 - cy_ * p0;
+        const R al = a.alpha, gb = -a.gamma_bar;
+        const R pr = a.precession ? 1.0 : 0.0;
+        const R r0 = (pr * p0 + q0 * al) * gb, r1 = (pr * p1 + q1 * al) * gb,
                 r2 = (pr * p2 + q2 * al) * gb;
-        if (a.kout) { a.kout[i] = r0; a.kout[n + i] = r1; a.kout[2 * n + i] = r2; }
-        if (a.hex_out) { a.hex_out[i] = h0; a.hex_out[n + i] = h1; a.hex_out[2 * n + i] = h2; }
-        if (a.heff_out) { a.heff_out[i] = e0; a.heff_out[n + i] = e1; a.heff_out[2 * n + i] = e2; }
+        if (a.kout) { a.kout[i] = (T)r0; a.kout[n + i] = (T)r1; a.kout[2 * n + i] = (T)r2; }
+        if (a.hex_out) { a.hex_out[i] = (T)h0; a.hex_out[n + i] = (T)h1; a.hex_out[2 * n + i] = (T)h2; }
+        if (a.heff_out) { a.heff_out[i] = (T)e0; a.heff_out[n + i] = (T)e1; a.heff_out[2 * n + i] = (T)e2; }
 
         if (MODE == MODE_HEUN_CORR) {
             // m = normalize(m0 + (k1 + k2) * (dt/2)), FP64 accumulation
             const double hd_ = a.half_dt;
-            const double v0 = (double)a.m0[i] + ((double)a.k1[i] + (double)r0) * hd_;
-            const double v1 = (double)a.m0[n + i] + ((double)a.k1[n + i] + (double)r1) * hd_;
-            const double v2 = (double)a.m0[2 * n + i] + ((double)a.k1[2 * n + i] + (double)r2) * hd_;
+            const double v0 = (double)a.m0[i] + ((double)a.k1[i] + r0) * hd_;
+            const double v1 = (double)a.m0[n + i] + ((double)a.k1[n + i] + r1) * hd_;
+            const double v2 = (double)a.m0[2 * n + i] + ((double)a.k1[2 * n + i] + r2) * hd_;
             const double nn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
             const double inv = nn > 0.0 ? 1.0 / nn : 0.0;
             a.m0[i] = (T)(v0 * inv); a.m0[n + i] = (T)(v1 * inv); a.m0[2 * n + i] = (T)(v2 * inv);
@@ -212,7 +215,8 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
                 const double E[6] = {71.0 / 57600.0, -71.0 / 16695.0, 71.0 / 1920.0,
                                      -17253.0 / 339200.0, 22.0 / 525.0, -1.0 / 40.0};
                 double er[3] = {0.0, 0.0, 0.0};
-                const double rr[3] = {(double)r0, (double)r1, (double)r2};
+                // the stored k7 (rounded to T) enters the error like the other stages
+                const double rr[3] = {(double)(T)r0, (double)(T)r1, (double)(T)r2};
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     double e = 0.0;
@@ -243,7 +247,7 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
             }
             const double coef = ms_i * a.vol * kMu0;
             acc[Q_EDEMAG] += -0.5 * coef * (m0d * (double)d0 + m1d * (double)d1 + m2d * (double)d2);
-            acc[Q_EEXT] += -coef * (m0d * (double)hex0 + m1d * (double)hex1 + m2d * (double)hex2);
+            acc[Q_EEXT] += -coef * (m0d * hx0 + m1d * hx1 + m2d * hx2);
             const double E0 = e0, E1 = e1, E2 = e2;
             acc[Q_HEFF2] = fmax(acc[Q_HEFF2], E0 * E0 + E1 * E1 + E2 * E2);
             const double D0 = d0, D1 = d1, D2 = d2;

@@ -338,3 +338,26 @@ def test_runtime_errors_are_reported():
     rc = lib.fullmag_fdm_backend_copy_field_f64(be.handle, nf.OBS_M, out.ctypes.data_as(nf._dp), 5)
     assert rc == nf.ERR_INVALID
     assert lib.fullmag_fdm_backend_last_error(be.handle) == b"out_len mismatch"
+
+
+@pytest.mark.parametrize("fft", ["register", "stockham"])
+@pytest.mark.parametrize("cells,prec", [((64, 16, 1), nf.PRECISION_DOUBLE), ((32, 16, 8), nf.PRECISION_DOUBLE),
+                                        ((32, 16, 8), nf.PRECISION_SINGLE), ((64, 32, 16), nf.PRECISION_SINGLE),
+                                        ((256, 64, 1), nf.PRECISION_DOUBLE)])
+def test_both_fft_paths_match_oracle(monkeypatch, fft, cells, prec):
+    """The register-FFT kernels (power-of-two lengths) and the shared-memory
+    Stockham kernels (any 2,3,5,7-smooth length; forced by FULLMAG_FDM_FFT)."""
+    if fft == "stockham":
+        monkeypatch.setenv("FULLMAG_FDM_FFT", "stockham")
+    else:
+        monkeypatch.delenv("FULLMAG_FDM_FFT", raising=False)
+    be, sim, _ = make_pair(cells, (2e-9, 2e-9, 2e-9), alpha=0.3, h_ext=(1e4, 0, 2e4), precision=prec,
+                           symmetric_kernel=True, seed=7)
+    err = _field_errors(be, sim.observe())
+    tol = 1e-13 if prec == nf.PRECISION_DOUBLE else 2e-6
+    for k, v in err.items():
+        assert v <= tol, (fft, k, v)
+    for _ in range(5):
+        be.step(2e-14)
+        sim.step(2e-14)
+    assert max_abs(be.copy_m(), sim.m) <= (1e-12 if prec == nf.PRECISION_DOUBLE else 1e-6)
