@@ -200,6 +200,7 @@ def run_ours(args):
 
     results = {}
     sampler_out = None
+    floor_dm = None
     for prec, tag in ((nf.PRECISION_DOUBLE, "fp64"), (nf.PRECISION_SINGLE, "fp32")):
         be = make(prec)
         stream = torch.cuda.ExternalStream(be.stream())
@@ -244,6 +245,11 @@ def run_ours(args):
         be.upload_m(m0)
         be.step_n(dt, ACCURACY_STEPS)
         m_acc = be.copy_m()
+        if tag == "fp64":
+            # sensitivity floor of the workload itself: FP64 from m0 rounded once to FP32
+            be.upload_m(m0.astype(np.float32).astype(np.float64))
+            be.step_n(dt, ACCURACY_STEPS)
+            floor_dm = float(np.abs(be.copy_m() - m_acc).max())
         results[tag] = dict(ms=ms, prof=prof, ms_e2e=ms_e2e, m=m_acc,
                             mem=be.memory_info()[0])
         be.close()
@@ -297,6 +303,7 @@ def run_ours(args):
             "fp64": {"value": v64, "ms_per_step": results["fp64"]["ms"] / K,
                      "speedup_fp32_over_fp64": v32 / v64, "kernels": kernels64},
             "max_dm_fp32_vs_fp64": max_dm, "max_dm_after_steps": ACCURACY_STEPS,
+            "fp64_sensitivity_to_one_fp32_rounding_of_m0": floor_dm,
             "e2e": {"value": e2e32, "unit": "cell-updates/s", "h2d_bytes_per_step": bi,
                     "d2h_bytes_per_step": bo,
                     "fp64_value": cells_job / (results["fp64"]["ms_e2e"] * 1e-3)},

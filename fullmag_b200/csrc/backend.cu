@@ -390,8 +390,10 @@ struct Impl {
     }
 
     static unsigned grid_cells(const Backend &b) {
-        return (unsigned)std::min<long long>((b.n + 255) / 256, (long long)b.red_blocks);
+        return (unsigned)std::min<long long>((b.n + 255) / 256, 148LL * 16);
     }
+    // stage kernels: block (32, 8) over (x, y), each thread marching along z
+    static dim3 stage_grid(const Backend &b) { return dim3((b.nx + 31) / 32, (b.ny + 7) / 8, 1); }
 
     // k = RHS(m, t); optional observables and diagnostics.
     static bool eval(Backend &b, const void *m, double t, void *kout, bool diag, bool obs) {
@@ -400,14 +402,11 @@ struct Impl {
         s.hex_out = obs ? (T *)b.hex : nullptr;
         s.heff_out = obs ? (T *)b.heff : nullptr;
         s.partials = diag ? b.partials : nullptr;
-        const unsigned g = diag ? (unsigned)b.red_blocks : grid_cells(b);
+        s.counter = b.counter;
+        s.out = b.d_out;
         {
             ProfScope p(b, "stage_eval");
-            k_stage<T, MODE_EVAL><<<g, 256, 0, b.stream>>>(s);
-        }
-        if (diag) {
-            ProfScope p(b, "reduce_finalize");
-            k_finalize<<<1, 256, 0, b.stream>>>(b.partials, b.red_blocks, b.d_out);
+            k_stage<T, MODE_EVAL><<<stage_grid(b), dim3(32, 8), 0, b.stream>>>(s);
         }
         return check_launch(b, "stage_eval");
     }
@@ -474,7 +473,7 @@ struct Impl {
         s.half_dt = 0.5 * dt;
         {
             ProfScope p(b, "stage_heun_corr");
-            k_stage<T, MODE_HEUN_CORR><<<grid_cells(b), 256, 0, b.stream>>>(s);
+            k_stage<T, MODE_HEUN_CORR><<<stage_grid(b), dim3(32, 8), 0, b.stream>>>(s);
         }
         if (!check_launch(b, "heun corrector")) return false;
         // fields, RHS (next k1) and diagnostics at the new state
@@ -525,16 +524,14 @@ struct Impl {
             StageArgs<T> s = stage_args(b, b.mstage, t + dt);
             s.kout = (T *)k[6];
             s.partials = b.partials;
+            s.counter = b.counter;
+            s.out = b.d_out;
             s.ke[0] = (const T *)k[0]; s.ke[1] = (const T *)k[2]; s.ke[2] = (const T *)k[3];
             s.ke[3] = (const T *)k[4]; s.ke[4] = (const T *)k[5];
             s.dt = dt;
             {
                 ProfScope p(b, "stage_dp45_last");
-                k_stage<T, MODE_DP45_LAST><<<b.red_blocks, 256, 0, b.stream>>>(s);
-            }
-            {
-                ProfScope p(b, "reduce_finalize");
-                k_finalize<<<1, 256, 0, b.stream>>>(b.partials, b.red_blocks, b.d_out);
+                k_stage<T, MODE_DP45_LAST><<<stage_grid(b), dim3(32, 8), 0, b.stream>>>(s);
             }
             if (!check_launch(b, "dp45 last stage") || !read_stats(b)) return false;
             const double err = std::sqrt(b.h_out[Q_ERR2]);
@@ -672,9 +669,10 @@ bool backend_alloc(Backend &b) {
         items.push_back({(void **)&b.d_lut, (size_t)256 * 256 * 8});
     }
     if (b.has_ms_map) items.push_back({(void **)&b.d_msmap, (size_t)b.n * 8});
-    b.red_blocks = (int)std::max<long long>(1, std::min<long long>((b.n + 255) / 256, 148LL * 8));
+    b.red_blocks = ((b.nx + 31) / 32) * ((b.ny + 7) / 8);  // blocks of the stage grid
     items.push_back({(void **)&b.partials, (size_t)NQ * b.red_blocks * 8});
     items.push_back({(void **)&b.d_out, (size_t)NQ * 8 + 64});
+    items.push_back({(void **)&b.counter, 64});
     size_t total = 0;
     for (auto &it : items) total += (it.bytes + 255) / 256 * 256;
     if (!cuda_ok(b, cudaMalloc(&b.arena, total), "cudaMalloc(arena)")) return false;

@@ -73,6 +73,7 @@ struct Backend {
     int red_blocks = 0;
     double *partials = nullptr;
     double *d_out = nullptr;
+    unsigned *counter = nullptr;  // blocks finished in the reducing stage kernel
     double *h_out = nullptr;  // pinned, NQ doubles
 
     // ---- per-kernel timing (extension API) ----

@@ -13,8 +13,10 @@
 
 namespace fm {
 
+// Per-line shared-memory region (tile, then the line's outputs), padded by one
+// element so that consecutive lines start in different banks.
 template <int L1, int L2> __host__ __device__ constexpr int line_region() {
-    return tile_elems(L1, L2) > L1 * L2 ? tile_elems(L1, L2) : L1 * L2;
+    return (tile_elems(L1, L2) > L1 * L2 ? tile_elems(L1, L2) : L1 * L2) + 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -174,18 +176,18 @@ __global__ void __launch_bounds__(128) k_zc_r(DemagArgs<T> a) {
     using C = cx<T>;
     constexpr int NZL = LZ / P;  // points per thread
     static_assert(P == 1 || P == 2, "z split");
-    const long long cols = (long long)a.nkx * a.Ly;
+    // nkx * Ly < 2^31 for every supported grid: 32-bit index math
+    const int cols = a.nkx * a.Ly;
     const int nz = a.nz, Ly = a.Ly, nkx = a.nkx;
     const long long cs = (long long)nz * nkx * Ly;  // component stride in S2
     const long long zs = (long long)nkx * Ly;
     const int h = (P == 2) ? (threadIdx.x & 1) : 0;
-    const long long span = ((cols * P + 127) / 128) * 128;  // whole pairs and warps iterate together
-    for (long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x; tid < span;
-         tid += (long long)gridDim.x * blockDim.x) {
-        const long long col = tid / P;
+    const int span = ((cols * P + 127) / 128) * 128;  // whole pairs and warps iterate together
+    for (int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < span; tid += gridDim.x * blockDim.x) {
+        const int col = tid / P;
         const bool valid = col < cols;
-        const int kx = valid ? (int)(col / Ly) : 0;
-        const int ky = valid ? (int)(col - (long long)kx * Ly) : 0;
+        const int kx = valid ? col / Ly : 0;
+        const int ky = valid ? col - kx * Ly : 0;
         C *base = a.s2 + (long long)kx * Ly + ky;
         C vx[NZL], vy[NZL], vz[NZL];
 #pragma unroll
