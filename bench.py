@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="FP32-mixed warm-up + K timed steps only (for profiler runs)")
     return ap.parse_args()
 
 
@@ -197,6 +199,24 @@ def run_ours(args):
         t = torch.tensor([x], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.kernels_only:
+        be = make(nf.PRECISION_SINGLE)
+        be.step_n(dt, warm)
+        stream = torch.cuda.ExternalStream(be.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        be.step_n(dt, K)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if rank == 0:
+            print(json.dumps({"mode": "kernels-only", "steps": K, "ms_per_step": ms / K,
+                              "value": n * K / (ms * 1e-3)}))
+        be.close()
+        return
 
     results = {}
     sampler_out = None
