@@ -80,6 +80,43 @@ int fullmag_fdm_newell_spectra(uint32_t nx, uint32_t ny, uint32_t nz, double dx,
                                double dz, int thin_film_2d, double *xx, double *yy,
                                double *zz, double *xy, double *xz, double *yz);
 
+/* Demag field H = -IFFT(N(k) FFT(Ms m)) without any device allocation.
+ *
+ * This entry point has no counterpart in the reference.  It serves callers
+ * that cannot allocate device memory themselves through this library: code
+ * running inside a host framework that owns the whole device-memory budget
+ * (every allocation must go through that framework's allocator), and
+ * latency-critical loops that must avoid the implicit device synchronisation
+ * of cudaMalloc / cudaFree.  The caller passes device pointers for the inputs
+ * and the output; the library allocates nothing.
+ *
+ *   octant : FP64 Newell octant [6][KZ][nx+1][ny+1] (components xx, yy, zz,
+ *            xy, xz, yz; KZ = nz + 1, or 1 for the thin-film form): the real
+ *            parts of the spectra fullmag_fdm_newell_spectra returns, at
+ *            kz <= nz (kz = 0 when thin), kx <= nx, ky <= ny;
+ *   m      : SoA [x[N], y[N], z[N]] FP64 unit vectors, every cell active;
+ *   ms     : uniform saturation magnetisation (A/m);
+ *   h      : SoA [3N] FP64 output;
+ *   stream : cudaStream_t to launch on (NULL = legacy default stream);
+ *   error_out / error_out_len : optional buffer for a failure message.
+ *
+ * Limits: 2nx and 2ny powers of two <= 1024, and 2nz <= 16 unless nz = 1 and
+ * thin_film_2d is set; the FFT work arrays must fit the library's fixed 32 MiB
+ * scratch array (every GPU that loads the library holds it until the process
+ * exits).  Larger grids are rejected with FULLMAG_FDM_ERR_INVALID and a message
+ * giving the bytes needed.
+ *
+ * The first call on a device resolves the scratch array's device address and
+ * fills the twiddle constants; make that first call outside any CUDA stream
+ * capture.  All calls share the one scratch array: calls that overlap on the
+ * GPU (different streams or threads without ordering) race.  Each call writes
+ * every scratch element it reads, so nothing has to start at zero. */
+int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uint32_t nz,
+                                        int thin_film_2d, const double *octant,
+                                        const double *m, double ms, double *h,
+                                        void *stream, char *error_out,
+                                        uint64_t error_out_len);
+
 #ifdef __cplusplus
 }
 #endif
