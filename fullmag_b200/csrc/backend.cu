@@ -167,7 +167,7 @@ struct Impl {
         if (!is_pow2(b.Lx) || !is_pow2(b.Ly) || b.Lx > maxxy || b.Ly > maxxy) return false;
         if (!b.thin && (!is_pow2(b.Lz) || b.Lz > maxz)) return false;
         const size_t sz = sizeof(C), maxs = 200 * 1024;
-        const int target = (dbl && b.Lx >= 512) ? 128 : 256;
+        const int target = 128;  // x passes: small blocks, several per SM
         bool ok = true;
         // x passes: lines_x complex lines (row pairs) of L2 threads
         with_split(b.Lx, [&](auto l1, auto l2) {
@@ -392,8 +392,10 @@ struct Impl {
     static unsigned grid_cells(const Backend &b) {
         return (unsigned)std::min<long long>((b.n + 255) / 256, 148LL * 16);
     }
-    // stage kernels: block (32, 8) over (x, y), each thread marching along z
-    static dim3 stage_grid(const Backend &b) { return dim3((b.nx + 31) / 32, (b.ny + 7) / 8, 1); }
+    // stage kernels: one thread per cell, block (32, 4, 2)
+    static dim3 stage_grid(const Backend &b) {
+        return dim3((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
+    }
 
     // k = RHS(m, t); optional observables and diagnostics.
     static bool eval(Backend &b, const void *m, double t, void *kout, bool diag, bool obs) {
@@ -406,7 +408,7 @@ struct Impl {
         s.out = b.d_out;
         {
             ProfScope p(b, "stage_eval");
-            k_stage<T, MODE_EVAL><<<stage_grid(b), dim3(32, 8), 0, b.stream>>>(s);
+            k_stage<T, MODE_EVAL><<<stage_grid(b), dim3(32, 4, 2), 0, b.stream>>>(s);
         }
         return check_launch(b, "stage_eval");
     }
@@ -473,7 +475,7 @@ struct Impl {
         s.half_dt = 0.5 * dt;
         {
             ProfScope p(b, "stage_heun_corr");
-            k_stage<T, MODE_HEUN_CORR><<<stage_grid(b), dim3(32, 8), 0, b.stream>>>(s);
+            k_stage<T, MODE_HEUN_CORR><<<stage_grid(b), dim3(32, 4, 2), 0, b.stream>>>(s);
         }
         if (!check_launch(b, "heun corrector")) return false;
         // fields, RHS (next k1) and diagnostics at the new state
@@ -531,7 +533,7 @@ struct Impl {
             s.dt = dt;
             {
                 ProfScope p(b, "stage_dp45_last");
-                k_stage<T, MODE_DP45_LAST><<<stage_grid(b), dim3(32, 8), 0, b.stream>>>(s);
+                k_stage<T, MODE_DP45_LAST><<<stage_grid(b), dim3(32, 4, 2), 0, b.stream>>>(s);
             }
             if (!check_launch(b, "dp45 last stage") || !read_stats(b)) return false;
             const double err = std::sqrt(b.h_out[Q_ERR2]);
@@ -669,7 +671,7 @@ bool backend_alloc(Backend &b) {
         items.push_back({(void **)&b.d_lut, (size_t)256 * 256 * 8});
     }
     if (b.has_ms_map) items.push_back({(void **)&b.d_msmap, (size_t)b.n * 8});
-    b.red_blocks = ((b.nx + 31) / 32) * ((b.ny + 7) / 8);  // blocks of the stage grid
+    b.red_blocks = ((b.nx + 31) / 32) * ((b.ny + 3) / 4) * ((b.nz + 1) / 2);  // stage grid blocks
     items.push_back({(void **)&b.partials, (size_t)NQ * b.red_blocks * 8});
     items.push_back({(void **)&b.d_out, (size_t)NQ * 8 + 64});
     items.push_back({(void **)&b.counter, 64});

@@ -52,16 +52,24 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
     fft4step<L1, L2, false, false, true>(t, tw, line, in, out);
     __syncthreads();
     const int nkx = a.nkx;
-    for (int u = threadIdx.x; u < nkx * RB; u += blockDim.x) {
-        const int k = u / RB, r = u - k * RB, y = y0 + r;
-        if (y >= ny) continue;
+    C *s1row = a.s1 + ((long long)c * a.nz + z) * nkx * ny;
+    auto emit = [&](int k, int r) {
+        const int y = y0 + r;
+        if (y >= ny) return;
         const C *ln = region + (r >> 1) * TE;
         const C zk = ln[k];
         const C zm = ln[k == 0 ? 0 : L - k];
         C o;
         if ((r & 1) == 0) { o.x = T(0.5) * (zk.x + zm.x); o.y = T(0.5) * (zk.y - zm.y); }
         else { o.x = T(0.5) * (zk.y + zm.y); o.y = T(-0.5) * (zk.x - zm.x); }
-        a.s1[(((long long)c * a.nz + z) * nkx + k) * ny + y] = o;
+        s1row[(long long)k * ny + y] = o;
+    };
+    if (blockDim.x % RB == 0) {
+        // each thread keeps its row; k advances by blockDim / RB (no division in the loop)
+        const int r = threadIdx.x % RB, kstep = blockDim.x / RB;
+        for (int k = threadIdx.x / RB; k < nkx; k += kstep) emit(k, r);
+    } else {
+        for (int u = threadIdx.x; u < nkx * RB; u += blockDim.x) emit(u / RB, u % RB);
     }
 }
 
@@ -81,15 +89,14 @@ __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
     for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twx[k];
     // Z[k] = A[k] + i B[k] (k <= nx), Z[L-k] = conj(A[k]) + i conj(B[k]); DC and
     // Nyquist taken as real.  Row pairs (A, B) sit in adjacent lanes.
-    const int total = nkx * RB;
-    const int span = (total + 31) / 32 * 32;
-    for (int u = threadIdx.x; u < span; u += blockDim.x) {
-        const int k = u / RB, r = u - k * RB, y = y0 + r;
+    const C *s1row = a.s1 + ((long long)c * a.nz + z) * nkx * ny;
+    auto gather = [&](int k, int r, bool ok) {
+        const int y = y0 + r;
         C v = mk<T>(0, 0);
-        if (u < total && y < ny) v = a.s1[(((long long)c * a.nz + z) * nkx + k) * ny + y];
+        if (ok && y < ny) v = s1row[(long long)k * ny + y];
         const T bx = __shfl_down_sync(0xffffffffu, v.x, 1);
         const T by = __shfl_down_sync(0xffffffffu, v.y, 1);
-        if (u < total && (r & 1) == 0) {
+        if (ok && (r & 1) == 0) {
             C A = v, B = mk<T>(bx, by);
             C *ln = region + (r >> 1) * TE;
             if (k == 0 || k == nx) {
@@ -99,6 +106,19 @@ __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
                 ln[L - k] = mk<T>(A.x + B.y, -A.y + B.x);
             }
         }
+    };
+    if (blockDim.x % RB == 0) {
+        // fixed row per thread, warp-uniform trip count (the shuffle needs whole warps)
+        const int r = threadIdx.x % RB, kstep = blockDim.x / RB, k0 = threadIdx.x / RB;
+        const int iters = (nkx + kstep - 1) / kstep;
+        for (int it = 0; it < iters; ++it) {
+            const int k = k0 + it * kstep;
+            gather(k < nkx ? k : 0, r, k < nkx);
+        }
+    } else {
+        const int total = nkx * RB;
+        const int span = (total + 31) / 32 * 32;
+        for (int u = threadIdx.x; u < span; u += blockDim.x) gather(u / RB, u % RB, u < total);
     }
     __syncthreads();
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;

@@ -143,11 +143,23 @@ __device__ __forceinline__ void block_reduce_final(double (&acc)[NQ], double *pa
     __threadfence();
     for (int q = 0; q < NQ; ++q) {
         const bool mx = q_is_max(q);
-        double v = 0.0;
-        for (int b = tid; b < nblocks; b += nthr) {
-            const double w = __ldcg(&partials[(long long)q * nblocks + b]);
-            v = mx ? fmax(v, w) : v + w;
+        const double *pq = partials + (long long)q * nblocks;
+        // four independent accumulators per thread, combined in a fixed order
+        double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+        int b = tid;
+        for (; b + 3 * nthr < nblocks; b += 4 * nthr) {
+            const double w0 = __ldcg(pq + b), w1 = __ldcg(pq + b + nthr);
+            const double w2 = __ldcg(pq + b + 2 * nthr), w3 = __ldcg(pq + b + 3 * nthr);
+            v0 = mx ? fmax(v0, w0) : v0 + w0;
+            v1 = mx ? fmax(v1, w1) : v1 + w1;
+            v2 = mx ? fmax(v2, w2) : v2 + w2;
+            v3 = mx ? fmax(v3, w3) : v3 + w3;
         }
+        for (; b < nblocks; b += nthr) {
+            const double w = __ldcg(pq + b);
+            v0 = mx ? fmax(v0, w) : v0 + w;
+        }
+        double v = mx ? fmax(fmax(v0, v1), fmax(v2, v3)) : (v0 + v1) + (v2 + v3);
         v = warp_reduce(v, mx);
         __syncthreads();
         if (lane == 0) sred[0][warp] = v;
@@ -161,11 +173,11 @@ __device__ __forceinline__ void block_reduce_final(double (&acc)[NQ], double *pa
     if (tid == 0) *counter = 0u;
 }
 
-// One thread per (x, y) column marching along z: the z neighbours of the
-// state come from registers (prev / cur / next), x and y neighbours from
-// global memory (L1 / L2).  Block (32, 8), grid (ceil(nx/32), ceil(ny/8)).
+// One thread per cell; block (32, 4, 2), grid (ceil(nx/32), ceil(ny/4),
+// ceil(nz/2)).  x/y neighbours mostly hit L1, z neighbours L2; many small
+// independent threads keep enough loads in flight to stream HBM.
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
+__global__ void __launch_bounds__(256, 3) k_stage(StageArgs<T> a) {
     using R = double;
     double acc[NQ];
 #pragma unroll
@@ -175,167 +187,138 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
     const long long sxy = (long long)nx * ny;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z * blockDim.z + threadIdx.z;
     const T *mx = a.m, *my = a.m + n, *mz = a.m + 2 * n;
-    const double sinv = (a.ac_omega != 0.0) ? sin(a.t * a.ac_omega) : 0.0;
-    const double hx0 = a.has_ext ? a.hext[0] + a.hac[0] * sinv : 0.0;
-    const double hx1 = a.has_ext ? a.hext[1] + a.hac[1] * sinv : 0.0;
-    const double hx2 = a.has_ext ? a.hext[2] + a.hac[2] * sinv : 0.0;
     const bool masked = a.mask || a.ms_map;
-    const R ix2 = a.dinv[0], iy2 = a.dinv[1], iz2 = a.dinv[2];
 
-    if (x < nx && y < ny) {
-        const long long i0 = (long long)y * nx + x;
-        // sliding window along z: (value, active) of z-1, z, z+1
-        R pcx = 0, pcy = 0, pcz = 0, ccx, ccy, ccz, ncx = 0, ncy = 0, ncz = 0;
-        bool pact = false, cact, nact = false;
-        double ms_c;
-        ccx = mx[i0]; ccy = my[i0]; ccz = mz[i0];
-        cact = st_active(a, i0, ms_c);
-        for (int z = 0; z < nz; ++z) {
-            const long long i = i0 + (long long)z * sxy;
-            double ms_n = 0.0;
-            if (z + 1 < nz) {
-                const long long j = i + sxy;
-                ncx = mx[j]; ncy = my[j]; ncz = mz[j];
-                nact = st_active(a, j, ms_n);
-            } else {
-                nact = false;
-            }
-            const double ms_i = ms_c;
-            if (!cact) {
-                if (a.kout) { a.kout[i] = T(0); a.kout[n + i] = T(0); a.kout[2 * n + i] = T(0); }
-                if (a.hex_out) { a.hex_out[i] = T(0); a.hex_out[n + i] = T(0); a.hex_out[2 * n + i] = T(0); }
-                if (a.heff_out) { a.heff_out[i] = T(0); a.heff_out[n + i] = T(0); a.heff_out[2 * n + i] = T(0); }
-                if (MODE == MODE_HEUN_CORR) { a.m0[i] = T(0); a.m0[n + i] = T(0); a.m0[2 * n + i] = T(0); }
-            } else {
-                const R cx_ = ccx, cy_ = ccy, cz_ = ccz;
-                // in-plane neighbours: clamped at the edge, inactive -> centre
-                long long nb[4];
-                nb[0] = x < nx - 1 ? i + 1 : i;    // xp
-                nb[1] = x > 0 ? i - 1 : i;         // xm
-                nb[2] = y < ny - 1 ? i + nx : i;   // yp
-                nb[3] = y > 0 ? i - nx : i;        // ym
-                if (masked) {
+    if (x < nx && y < ny && z < nz) {
+        const long long i = ((long long)z * ny + y) * nx + x;
+        double ms_i;
+        if (!st_active(a, i, ms_i)) {
+            if (a.kout) { a.kout[i] = T(0); a.kout[n + i] = T(0); a.kout[2 * n + i] = T(0); }
+            if (a.hex_out) { a.hex_out[i] = T(0); a.hex_out[n + i] = T(0); a.hex_out[2 * n + i] = T(0); }
+            if (a.heff_out) { a.heff_out[i] = T(0); a.heff_out[n + i] = T(0); a.heff_out[2 * n + i] = T(0); }
+            if (MODE == MODE_HEUN_CORR) { a.m0[i] = T(0); a.m0[n + i] = T(0); a.m0[2 * n + i] = T(0); }
+        } else {
+            // neighbours: clamped at the grid edge, inactive -> centre (lib.rs:2255-2286)
+            long long nb[6];
+            nb[0] = x < nx - 1 ? i + 1 : i;     // xp
+            nb[1] = x > 0 ? i - 1 : i;          // xm
+            nb[2] = y < ny - 1 ? i + nx : i;    // yp
+            nb[3] = y > 0 ? i - nx : i;         // ym
+            nb[4] = z < nz - 1 ? i + sxy : i;   // zp
+            nb[5] = z > 0 ? i - sxy : i;        // zm
+            if (masked) {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        double msq;
-                        if (!st_active(a, nb[q], msq)) nb[q] = i;
+                for (int q = 0; q < 6; ++q) {
+                    double msq;
+                    if (!st_active(a, nb[q], msq)) nb[q] = i;
+                }
+            }
+            const R c3[3] = {(R)mx[i], (R)my[i], (R)mz[i]};
+            const T *comp[3] = {mx, my, mz};
+            R hxc[3] = {0.0, 0.0, 0.0};
+            if (a.enable_exchange) {
+                const R ix2 = a.dinv[0], iy2 = a.dinv[1], iz2 = a.dinv[2];
+                if (!a.region) {
+                    const R pref = 2.0 * a.aex / (kMu0 * ms_i);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const T *f = comp[c];
+                        const R lap = ((R)f[nb[0]] - 2.0 * c3[c] + (R)f[nb[1]]) * ix2 +
+                                      ((R)f[nb[2]] - 2.0 * c3[c] + (R)f[nb[3]]) * iy2 +
+                                      ((R)f[nb[4]] - 2.0 * c3[c] + (R)f[nb[5]]) * iz2;
+                        hxc[c] = lap * pref;
+                    }
+                } else {
+                    const R pref = 2.0 / (kMu0 * ms_i);
+                    const uint32_t rc = a.region[i];
+                    R aq[6];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) aq[q] = a.lut[(size_t)rc * 256 + a.region[nb[q]]];
+                    const R inv[3] = {ix2, iy2, iz2};
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        // order of exchange_fp64.cu:102-112: xp, xm, yp, ym, zp, zm
+                        const T *f = comp[c];
+                        R sm = 0.0;
+#pragma unroll
+                        for (int q = 0; q < 6; ++q) sm += aq[q] * ((R)f[nb[q]] - c3[c]) * inv[q >> 1];
+                        hxc[c] = pref * sm;
                     }
                 }
-                R vxp[3] = {(R)mx[nb[0]], (R)my[nb[0]], (R)mz[nb[0]]};
-                R vxm[3] = {(R)mx[nb[1]], (R)my[nb[1]], (R)mz[nb[1]]};
-                R vyp[3] = {(R)mx[nb[2]], (R)my[nb[2]], (R)mz[nb[2]]};
-                R vym[3] = {(R)mx[nb[3]], (R)my[nb[3]], (R)mz[nb[3]]};
-                const bool zp_ok = (z + 1 < nz) && nact, zm_ok = (z > 0) && pact;
-                R vzp[3] = {zp_ok ? ncx : cx_, zp_ok ? ncy : cy_, zp_ok ? ncz : cz_};
-                R vzm[3] = {zm_ok ? pcx : cx_, zm_ok ? pcy : cy_, zm_ok ? pcz : cz_};
-                const R c3[3] = {cx_, cy_, cz_};
-                R hxc[3] = {0.0, 0.0, 0.0};
+            }
+            const double sinv = (a.ac_omega != 0.0) ? sin(a.t * a.ac_omega) : 0.0;
+            const R hx0 = a.has_ext ? a.hext[0] + a.hac[0] * sinv : 0.0;
+            const R hx1 = a.has_ext ? a.hext[1] + a.hac[1] * sinv : 0.0;
+            const R hx2 = a.has_ext ? a.hext[2] + a.hac[2] * sinv : 0.0;
+            const R cx_ = c3[0], cy_ = c3[1], cz_ = c3[2];
+            const R h0 = hxc[0], h1 = hxc[1], h2 = hxc[2];
+            R d0 = 0.0, d1 = 0.0, d2 = 0.0;
+            if (a.enable_demag) { d0 = a.hd[i]; d1 = a.hd[n + i]; d2 = a.hd[2 * n + i]; }
+            const R e0 = (h0 + d0) + hx0, e1 = (h1 + d1) + hx1, e2 = (h2 + d2) + hx2;
+            // Gilbert RHS: -gamma_bar (m x H + alpha m x (m x H))
+            const R p0 = cy_ * e2 - cz_ * e1, p1 = cz_ * e0 - cx_ * e2, p2 = cx_ * e1 - cy_ * e0;
+            const R q0 = cy_ * p2 - cz_ * p1, q1 = cz_ * p0 - cx_ * p2, q2 = cx_ * p1 - cy_ * p0;
+            const R al = a.alpha, gb = -a.gamma_bar;
+            const R pr = a.precession ? 1.0 : 0.0;
+            const R r0 = (pr * p0 + q0 * al) * gb, r1 = (pr * p1 + q1 * al) * gb,
+                    r2 = (pr * p2 + q2 * al) * gb;
+            if (a.kout) { a.kout[i] = (T)r0; a.kout[n + i] = (T)r1; a.kout[2 * n + i] = (T)r2; }
+            if (a.hex_out) { a.hex_out[i] = (T)h0; a.hex_out[n + i] = (T)h1; a.hex_out[2 * n + i] = (T)h2; }
+            if (a.heff_out) { a.heff_out[i] = (T)e0; a.heff_out[n + i] = (T)e1; a.heff_out[2 * n + i] = (T)e2; }
+            if (MODE == MODE_HEUN_CORR) {
+                // m = normalize(m0 + (k1 + k2) * (dt/2)), FP64 accumulation
+                const double hd_ = a.half_dt;
+                const double v0 = (double)a.m0[i] + ((double)a.k1[i] + r0) * hd_;
+                const double v1 = (double)a.m0[n + i] + ((double)a.k1[n + i] + r1) * hd_;
+                const double v2 = (double)a.m0[2 * n + i] + ((double)a.k1[2 * n + i] + r2) * hd_;
+                const double nn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+                const double inv = nn > 0.0 ? 1.0 / nn : 0.0;
+                a.m0[i] = (T)(v0 * inv); a.m0[n + i] = (T)(v1 * inv); a.m0[2 * n + i] = (T)(v2 * inv);
+            }
+            if (a.partials) {
+                if (MODE == MODE_DP45_LAST) {
+                    // err = dt * (E1 k1 + E3 k3 + E4 k4 + E5 k5 + E6 k6 + E7 k7), lib.rs:1653-1674
+                    const double E[6] = {71.0 / 57600.0, -71.0 / 16695.0, 71.0 / 1920.0,
+                                         -17253.0 / 339200.0, 22.0 / 525.0, -1.0 / 40.0};
+                    // the stored k7 (rounded to T) enters the error like the other stages
+                    const double rr[3] = {(double)(T)r0, (double)(T)r1, (double)(T)r2};
+                    double er[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        double e = 0.0;
+#pragma unroll
+                        for (int st = 0; st < 5; ++st) e += E[st] * (double)a.ke[st][c * n + i];
+                        e += E[5] * rr[c];
+                        er[c] = e * a.dt;
+                    }
+                    acc[Q_ERR2] = fmax(acc[Q_ERR2], er[0] * er[0] + er[1] * er[1] + er[2] * er[2]);
+                }
                 if (a.enable_exchange) {
-                    if (!a.region) {
-                        const R pref = 2.0 * a.aex / (kMu0 * ms_i);
+                    // forward pairs (x+1, y+1, z+1) inside the grid, both active
+                    const bool has[3] = {x + 1 < nx, y + 1 < ny, z + 1 < nz};
+                    const long long fw[3] = {i + 1, i + nx, i + sxy};
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            const R lap = (vxp[c] - 2.0 * c3[c] + vxm[c]) * ix2 +
-                                          (vyp[c] - 2.0 * c3[c] + vym[c]) * iy2 +
-                                          (vzp[c] - 2.0 * c3[c] + vzm[c]) * iz2;
-                            hxc[c] = lap * pref;
-                        }
-                    } else {
-                        const R pref = 2.0 / (kMu0 * ms_i);
-                        const uint32_t rc = a.region[i];
-                        const long long nzp = zp_ok ? i + sxy : i, nzm = zm_ok ? i - sxy : i;
-                        const R axp = a.lut[(size_t)rc * 256 + a.region[nb[0]]];
-                        const R axm = a.lut[(size_t)rc * 256 + a.region[nb[1]]];
-                        const R ayp = a.lut[(size_t)rc * 256 + a.region[nb[2]]];
-                        const R aym = a.lut[(size_t)rc * 256 + a.region[nb[3]]];
-                        const R azp = a.lut[(size_t)rc * 256 + a.region[nzp]];
-                        const R azm = a.lut[(size_t)rc * 256 + a.region[nzm]];
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            // order of exchange_fp64.cu:102-112: xp, xm, yp, ym, zp, zm
-                            R sm = 0.0;
-                            sm += axp * (vxp[c] - c3[c]) * ix2;
-                            sm += axm * (vxm[c] - c3[c]) * ix2;
-                            sm += ayp * (vyp[c] - c3[c]) * iy2;
-                            sm += aym * (vym[c] - c3[c]) * iy2;
-                            sm += azp * (vzp[c] - c3[c]) * iz2;
-                            sm += azm * (vzm[c] - c3[c]) * iz2;
-                            hxc[c] = pref * sm;
-                        }
+                    for (int q = 0; q < 3; ++q) {
+                        if (!has[q]) continue;
+                        const long long j = fw[q];
+                        double msj;
+                        if (masked && !st_active(a, j, msj)) continue;
+                        const double coeff = a.region ? a.lut[(size_t)a.region[i] * 256 + a.region[j]] * a.vol
+                                                      : a.aex * a.vol;
+                        const double ddx = (double)mx[j] - cx_, ddy = (double)my[j] - cy_,
+                                     ddz = (double)mz[j] - cz_;
+                        acc[Q_EEX] += coeff * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[q];
                     }
                 }
-                const R h0 = hxc[0], h1 = hxc[1], h2 = hxc[2];
-                R d0 = 0.0, d1 = 0.0, d2 = 0.0;
-                if (a.enable_demag) { d0 = a.hd[i]; d1 = a.hd[n + i]; d2 = a.hd[2 * n + i]; }
-                const R e0 = (h0 + d0) + hx0, e1 = (h1 + d1) + hx1, e2 = (h2 + d2) + hx2;
-                // Gilbert RHS: -gamma_bar (m x H + alpha m x (m x H))
-                const R p0 = cy_ * e2 - cz_ * e1, p1 = cz_ * e0 - cx_ * e2, p2 = cx_ * e1 - cy_ * e0;
-                const R q0 = cy_ * p2 - cz_ * p1, q1 = cz_ * p0 - cx_ * p2, q2 = cx_ * p1 - cy_ * p0;
-                const R al = a.alpha, gb = -a.gamma_bar;
-                const R pr = a.precession ? 1.0 : 0.0;
-                const R r0 = (pr * p0 + q0 * al) * gb, r1 = (pr * p1 + q1 * al) * gb,
-                        r2 = (pr * p2 + q2 * al) * gb;
-                if (a.kout) { a.kout[i] = (T)r0; a.kout[n + i] = (T)r1; a.kout[2 * n + i] = (T)r2; }
-                if (a.hex_out) { a.hex_out[i] = (T)h0; a.hex_out[n + i] = (T)h1; a.hex_out[2 * n + i] = (T)h2; }
-                if (a.heff_out) { a.heff_out[i] = (T)e0; a.heff_out[n + i] = (T)e1; a.heff_out[2 * n + i] = (T)e2; }
-                if (MODE == MODE_HEUN_CORR) {
-                    // m = normalize(m0 + (k1 + k2) * (dt/2)), FP64 accumulation
-                    const double hd_ = a.half_dt;
-                    const double v0 = (double)a.m0[i] + ((double)a.k1[i] + r0) * hd_;
-                    const double v1 = (double)a.m0[n + i] + ((double)a.k1[n + i] + r1) * hd_;
-                    const double v2 = (double)a.m0[2 * n + i] + ((double)a.k1[2 * n + i] + r2) * hd_;
-                    const double nn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-                    const double inv = nn > 0.0 ? 1.0 / nn : 0.0;
-                    a.m0[i] = (T)(v0 * inv); a.m0[n + i] = (T)(v1 * inv); a.m0[2 * n + i] = (T)(v2 * inv);
-                }
-                if (a.partials) {
-                    if (MODE == MODE_DP45_LAST) {
-                        // err = dt * (E1 k1 + E3 k3 + E4 k4 + E5 k5 + E6 k6 + E7 k7), lib.rs:1653-1674
-                        const double E[6] = {71.0 / 57600.0, -71.0 / 16695.0, 71.0 / 1920.0,
-                                             -17253.0 / 339200.0, 22.0 / 525.0, -1.0 / 40.0};
-                        // the stored k7 (rounded to T) enters the error like the other stages
-                        const double rr[3] = {(double)(T)r0, (double)(T)r1, (double)(T)r2};
-                        double er[3];
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            double e = 0.0;
-#pragma unroll
-                            for (int st = 0; st < 5; ++st) e += E[st] * (double)a.ke[st][c * n + i];
-                            e += E[5] * rr[c];
-                            er[c] = e * a.dt;
-                        }
-                        acc[Q_ERR2] = fmax(acc[Q_ERR2], er[0] * er[0] + er[1] * er[1] + er[2] * er[2]);
-                    }
-                    if (a.enable_exchange) {
-                        // forward pairs (x+1, y+1, z+1) inside the grid, both active
-                        const bool has[3] = {x + 1 < nx, y + 1 < ny, z + 1 < nz};
-                        const long long fw[3] = {i + 1, i + nx, i + sxy};
-#pragma unroll
-                        for (int q = 0; q < 3; ++q) {
-                            if (!has[q]) continue;
-                            const long long j = fw[q];
-                            double msj;
-                            if (masked && !st_active(a, j, msj)) continue;
-                            const double coeff = a.region ? a.lut[(size_t)a.region[i] * 256 + a.region[j]] * a.vol
-                                                          : a.aex * a.vol;
-                            const double ddx = (q == 0 ? vxp[0] : q == 1 ? vyp[0] : (double)ncx) - cx_;
-                            const double ddy = (q == 0 ? vxp[1] : q == 1 ? vyp[1] : (double)ncy) - cy_;
-                            const double ddz = (q == 0 ? vxp[2] : q == 1 ? vyp[2] : (double)ncz) - cz_;
-                            acc[Q_EEX] += coeff * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[q];
-                        }
-                    }
-                    const double coef = ms_i * a.vol * kMu0;
-                    acc[Q_EDEMAG] += -0.5 * coef * (cx_ * d0 + cy_ * d1 + cz_ * d2);
-                    acc[Q_EEXT] += -coef * (cx_ * hx0 + cy_ * hx1 + cz_ * hx2);
-                    acc[Q_HEFF2] = fmax(acc[Q_HEFF2], e0 * e0 + e1 * e1 + e2 * e2);
-                    acc[Q_HD2] = fmax(acc[Q_HD2], d0 * d0 + d1 * d1 + d2 * d2);
-                    acc[Q_RHS2] = fmax(acc[Q_RHS2], r0 * r0 + r1 * r1 + r2 * r2);
-                }
+                const double coef = ms_i * a.vol * kMu0;
+                acc[Q_EDEMAG] += -0.5 * coef * (cx_ * d0 + cy_ * d1 + cz_ * d2);
+                acc[Q_EEXT] += -coef * (cx_ * hx0 + cy_ * hx1 + cz_ * hx2);
+                acc[Q_HEFF2] = fmax(acc[Q_HEFF2], e0 * e0 + e1 * e1 + e2 * e2);
+                acc[Q_HD2] = fmax(acc[Q_HD2], d0 * d0 + d1 * d1 + d2 * d2);
+                acc[Q_RHS2] = fmax(acc[Q_RHS2], r0 * r0 + r1 * r1 + r2 * r2);
             }
-            // slide the window
-            pcx = ccx; pcy = ccy; pcz = ccz; pact = cact;
-            ccx = ncx; ccy = ncy; ccz = ncz; cact = nact; ms_c = ms_n;
         }
     }
     if (a.partials) block_reduce_final(acc, a.partials, a.counter, a.out);
