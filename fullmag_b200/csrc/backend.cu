@@ -246,10 +246,8 @@ struct Impl {
             {
                 ProfScope p(b, "demag_z_conv");
                 const long long cols = (long long)b.nkx * b.Ly;
-                const unsigned gz = (unsigned)std::min<long long>((cols + 127) / 128, 148LL * 64);
-                // one thread per column up to 3 x 8 (FP64) / 3 x 16 (FP32) z points,
-                // a thread pair (split by kz parity) above
-                const bool dbl = sizeof(T) == 8;
+                // one thread per column up to 3 x 8 z points, a thread pair (split by
+                // kz parity) above
                 const int P = (b.Lz > 8) ? 2 : 1;
                 const unsigned gz2 = (unsigned)std::min<long long>((cols * P + 127) / 128, 148LL * 64);
                 switch (b.Lz * 10 + P) {
@@ -260,7 +258,6 @@ struct Impl {
                     case 322: if constexpr (sizeof(T) == 4) k_zc_r<T, 32, 2><<<gz2, 128, 0, b.stream>>>(a); break;
                     default: break;
                 }
-                (void)gz;
             }
             with_split(b.Ly, [&](auto l1, auto l2) {
                 constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
@@ -374,6 +371,8 @@ struct Impl {
         s.dinv[1] = 1.0 / (b.dy * b.dy);
         s.dinv[2] = 1.0 / (b.dz * b.dz);
         s.aex = b.aex; s.ms = b.ms; s.ms_map = b.d_msmap;
+        s.ex_pref = 2.0 * b.aex / (kMu0 * b.ms);
+        s.ex_pref_lut = 2.0 / (kMu0 * b.ms);
         s.mask = b.d_mask; s.region = b.d_region; s.lut = b.d_lut;
         s.enable_exchange = b.enable_exchange; s.enable_demag = b.enable_demag;
         s.has_ext = b.has_ext;

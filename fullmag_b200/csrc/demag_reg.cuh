@@ -39,17 +39,22 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
     const int ya = y0 + 2 * q, yb = ya + 1, nx = a.nx, ny = a.ny;
     const long long rowa = ((long long)z * ny + ya) * nx, rowb = rowa + nx;
     C *line = region + q * TE;
+    // M = Ms m in the storage precision (Ms of the uniform material is exact in FP32)
+    const T msT = (T)a.ms;
     auto in = [&](int j) -> C {
         C v = mk<T>(0, 0);
-        if (j < nx) {
+        if (!a.mask && !a.ms_map) {
+            if (ya < ny) v.x = mc[rowa + j] * msT;
+            if (yb < ny) v.y = mc[rowb + j] * msT;
+        } else {
             double msi;
-            if (ya < ny && cell_active(a, rowa + j, msi)) v.x = (T)((double)mc[rowa + j] * msi);
-            if (yb < ny && cell_active(a, rowb + j, msi)) v.y = (T)((double)mc[rowb + j] * msi);
+            if (ya < ny && cell_active(a, rowa + j, msi)) v.x = mc[rowa + j] * (T)msi;
+            if (yb < ny && cell_active(a, rowb + j, msi)) v.y = mc[rowb + j] * (T)msi;
         }
         return v;
     };
     auto out = [&](int k, C v) { line[k] = v; };
-    fft4step<L1, L2, false, false, true>(t, tw, line, in, out);
+    fft4step<L1, L2, false, false, true, true>(t, tw, line, in, out);
     __syncthreads();
     const int nkx = a.nkx;
     C *s1row = a.s1 + ((long long)c * a.nz + z) * nkx * ny;
@@ -155,9 +160,9 @@ __global__ void __launch_bounds__(256) k_yf_r(DemagArgs<T> a) {
     const bool valid = g < total;
     const C *src = a.s1 + g * ny;
     C *dst = a.s2 + g * L;
-    auto in = [&](int j) -> C { return (valid && j < ny) ? src[j] : mk<T>(0, 0); };
+    auto in = [&](int j) -> C { return valid ? src[j] : mk<T>(0, 0); };
     auto out = [&](int k, C v) { if (valid) dst[k] = v; };
-    fft4step<L1, L2, false, false, false>(t, tw, region + q * TE, in, out);
+    fft4step<L1, L2, false, false, false, true>(t, tw, region + q * TE, in, out);
 }
 
 // y inverse (3-D): S2 -> S1, keeps y < ny
@@ -251,7 +256,7 @@ __global__ void __launch_bounds__(128) k_zc_r(DemagArgs<T> a) {
             for (int zz = 0; zz < NZL / 2; ++zz) {
                 // register selection by h without dynamic indexing
                 const int zlo = zz, zhi = zz + NZL / 2;
-                const int zmine = h ? zhi : zlo, zsend = h ? zlo : zhi;
+                const int zmine = h ? zhi : zlo;
                 C ox = h ? vx[zhi] : vx[zlo], oy = h ? vy[zhi] : vy[zlo], oz = h ? vz[zhi] : vz[zlo];
                 C sx = h ? vx[zlo] : vx[zhi], sy = h ? vy[zlo] : vy[zhi], sz = h ? vz[zlo] : vz[zhi];
                 if (h == 1) {
@@ -295,9 +300,9 @@ __global__ void __launch_bounds__(256) k_yc_r(DemagArgs<T> a) {
     const bool valid = kx < nkx;
     C *line = region + q * TE;
     C *g = a.s1 + ((long long)comp * nkx + kx) * ny;
-    auto in_g = [&](int j) -> C { return (valid && j < ny) ? g[j] : mk<T>(0, 0); };
+    auto in_g = [&](int j) -> C { return valid ? g[j] : mk<T>(0, 0); };
     auto out_s = [&](int k, C v) { line[k] = v; };
-    fft4step<L1, L2, false, false, true>(t, tw, line, in_g, out_s);
+    fft4step<L1, L2, false, false, true, true>(t, tw, line, in_g, out_s);
     __syncthreads();
     for (int u = threadIdx.x; u < KB * L; u += blockDim.x) {
         const int kl = u / L, ky = u - kl * L;

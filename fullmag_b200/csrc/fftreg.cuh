@@ -109,12 +109,19 @@ __host__ __device__ constexpr int tile_elems(int L1, int L2) { return L2 == 1 ? 
 // (barrier before the tile is written); ALIAS_OUT: out() writes memory the
 // tile overlaps (barrier before the outputs are written).  All threads of the
 // block must call this the same number of times (it contains barriers).
-template <int L1, int L2, bool INV, bool ALIAS_IN, bool ALIAS_OUT, typename C, class In, class Out>
+// HALF_IN: inputs j >= L/2 are known zero (zero padding); since j = t + L2 i
+// with t < L2, that is exactly i >= L1/2, so those registers are constant zero
+// and the first radix-2 stage of fft_reg folds away.
+template <int L1, int L2, bool INV, bool ALIAS_IN, bool ALIAS_OUT, bool HALF_IN = false, typename C,
+          class In, class Out>
 __device__ __forceinline__ void fft4step(int t, const C *__restrict__ tw, C *tile, In in, Out out) {
     constexpr int L = L1 * L2;
     C v[L1];
 #pragma unroll
-    for (int i = 0; i < L1; ++i) v[i] = in(t + L2 * i);
+    for (int i = 0; i < L1; ++i) {
+        if (HALF_IN && i >= L1 / 2) { v[i].x = 0; v[i].y = 0; }
+        else v[i] = in(t + L2 * i);
+    }
     fft_reg<L1, INV>(v);
     if constexpr (L2 == 1) {
         if (ALIAS_OUT) __syncthreads();

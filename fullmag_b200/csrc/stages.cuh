@@ -46,6 +46,8 @@ struct StageArgs {
     T idx2, idy2, idz2;             // 1/dx^2, 1/dy^2, 1/dz^2
     double dinv[3];                 // same, FP64 (energies)
     double aex, ms;                 // uniform A and Ms
+    double ex_pref;                 // 2 A / (mu0 Ms) for the uniform material
+    double ex_pref_lut;             // 2 / (mu0 Ms) for the uniform material (region LUT)
     const double *ms_map;           // optional per-cell Ms
     const uint8_t *mask;            // optional
     const uint32_t *region;         // optional
@@ -82,26 +84,6 @@ __device__ __forceinline__ double warp_reduce(double v, bool is_max) {
     return v;
 }
 
-// Reduce acc[NQ] over the block; thread 0 stores partials[q * gridDim.x + blockIdx.x].
-__device__ __forceinline__ void block_reduce_store(double (&acc)[NQ], double *partials) {
-    __shared__ double sred[NQ][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-        double v = warp_reduce(acc[q], q_is_max(q));
-        if (lane == 0) sred[q][warp] = v;
-    }
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            double v = lane < nw ? sred[q][lane] : 0.0;
-            v = warp_reduce(v, q_is_max(q));
-            if (lane == 0) partials[(long long)q * gridDim.x + blockIdx.x] = v;
-        }
-    }
-}
-
 template <typename T>
 __device__ __forceinline__ bool st_active(const StageArgs<T> &a, long long i, double &ms_i) {
     ms_i = a.ms_map ? a.ms_map[i] : a.ms;
@@ -114,8 +96,8 @@ __device__ __forceinline__ void block_reduce_final(double (&acc)[NQ], double *pa
                                                    unsigned *counter, double *out) {
     __shared__ double sred[NQ][32];
     __shared__ bool am_last;
-    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-    const int nthr = blockDim.x * blockDim.y;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthr = blockDim.x * blockDim.y * blockDim.z;
     const int lane = tid & 31, warp = tid >> 5, nw = (nthr + 31) >> 5;
     const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     const int nblocks = gridDim.x * gridDim.y * gridDim.z;
@@ -221,7 +203,7 @@ __global__ void __launch_bounds__(256, 3) k_stage(StageArgs<T> a) {
             if (a.enable_exchange) {
                 const R ix2 = a.dinv[0], iy2 = a.dinv[1], iz2 = a.dinv[2];
                 if (!a.region) {
-                    const R pref = 2.0 * a.aex / (kMu0 * ms_i);
+                    const R pref = a.ms_map ? 2.0 * a.aex / (kMu0 * ms_i) : a.ex_pref;
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const T *f = comp[c];
@@ -231,7 +213,7 @@ __global__ void __launch_bounds__(256, 3) k_stage(StageArgs<T> a) {
                         hxc[c] = lap * pref;
                     }
                 } else {
-                    const R pref = 2.0 / (kMu0 * ms_i);
+                    const R pref = a.ms_map ? 2.0 / (kMu0 * ms_i) : a.ex_pref_lut;
                     const uint32_t rc = a.region[i];
                     R aq[6];
 #pragma unroll
@@ -273,8 +255,14 @@ __global__ void __launch_bounds__(256, 3) k_stage(StageArgs<T> a) {
                 const double v0 = (double)a.m0[i] + ((double)a.k1[i] + r0) * hd_;
                 const double v1 = (double)a.m0[n + i] + ((double)a.k1[n + i] + r1) * hd_;
                 const double v2 = (double)a.m0[2 * n + i] + ((double)a.k1[2 * n + i] + r2) * hd_;
-                const double nn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-                const double inv = nn > 0.0 ? 1.0 / nn : 0.0;
+                const double n2 = v0 * v0 + v1 * v1 + v2 * v2;
+                double inv;
+                if (sizeof(T) == 8) {
+                    const double nn = sqrt(n2);  // FP64 path: 1/sqrt rounded like the reference
+                    inv = nn > 0.0 ? 1.0 / nn : 0.0;
+                } else {
+                    inv = n2 > 0.0 ? rsqrt(n2) : 0.0;  // result is stored in FP32
+                }
                 a.m0[i] = (T)(v0 * inv); a.m0[n + i] = (T)(v1 * inv); a.m0[2 * n + i] = (T)(v2 * inv);
             }
             if (a.partials) {
@@ -373,34 +361,17 @@ __global__ void __launch_bounds__(256) k_combine(CombineArgs<T> a) {
             }
             v[comp] = (double)a.m0[o] + inc;
         }
-        const double nn = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-        const double inv = nn > 0.0 ? 1.0 / nn : 0.0;
+        const double n2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        double inv;
+        if (sizeof(T) == 8) {
+            const double nn = sqrt(n2);
+            inv = nn > 0.0 ? 1.0 / nn : 0.0;
+        } else {
+            inv = n2 > 0.0 ? rsqrt(n2) : 0.0;
+        }
         a.out[i] = (T)(v[0] * inv);
         a.out[n + i] = (T)(v[1] * inv);
         a.out[2 * n + i] = (T)(v[2] * inv);
-    }
-}
-
-// Deterministic final reduction of the per-block partials: one block.
-__global__ void __launch_bounds__(256) k_finalize(const double *partials, int nblocks, double *out) {
-    __shared__ double sred[32];
-    for (int q = 0; q < NQ; ++q) {
-        const bool mx = q_is_max(q);
-        double v = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-            const double w = partials[(long long)q * nblocks + b];
-            v = mx ? fmax(v, w) : v + w;
-        }
-        v = warp_reduce(v, mx);
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        if (lane == 0) sred[warp] = v;
-        __syncthreads();
-        if (warp == 0) {
-            double w = lane < nw ? sred[lane] : 0.0;
-            w = warp_reduce(w, mx);
-            if (lane == 0) out[q] = w;
-        }
-        __syncthreads();
     }
 }
 
