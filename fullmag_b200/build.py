@@ -59,14 +59,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
     env = dict(os.environ)
     # nvcc must use the system host compiler
     host_cxx = shutil.which("g++", path="/usr/bin") or "g++"
+    cmds = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = [nvcc(), *NVCC_FLAGS, "-ccbin", host_cxx, "-I", os.path.join(ROOT, "include"),
-               "-I", CSRC, "-c", src, "-o", obj]
+        cmds.append([nvcc(), *NVCC_FLAGS, "-ccbin", host_cxx, "-I", os.path.join(ROOT, "include"),
+                     "-I", CSRC, "-c", src, "-o", obj])
+        objs.append(obj)
+    # translation units compile concurrently; any failure stops the build
+    procs = []
+    for cmd in cmds:
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True, env=env)
-        objs.append(obj)
+        procs.append((cmd, subprocess.Popen(cmd, env=env)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     tmp = LIB + ".tmp"
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-ccbin", host_cxx,
            "-Xlinker", f"-soname,{SONAME}", "-o", tmp, *objs, "-lpthread"]

@@ -247,6 +247,13 @@ bool create_impl(Backend &b, const fullmag_fdm_plan_desc *plan, const fullmag_fd
         // power-of-two lengths (both FFT paths are covered by the parity tests)
         const char *f = std::getenv("FULLMAG_FDM_FFT");
         b.force_stockham = f && std::strcmp(f, "stockham") == 0;
+        const char *yz = std::getenv("FULLMAG_FDM_YZ");
+        b.want_yz = yz && std::strcmp(yz, "fused") == 0;
+        const char *yzp = std::getenv("FULLMAG_FDM_YZ_P");
+        if (yzp) {
+            const int v = std::atoi(yzp);
+            if (v == 1 || v == 2 || v == 4 || v == 8) b.yz_min_P = v;
+        }
     }
     if (b.has_mask) b.mask_host.assign(plan->active_mask, plan->active_mask + b.n);
 

@@ -22,6 +22,7 @@
 #include "backend_impl.hpp"
 #include "demag.cuh"
 #include "demag_reg.cuh"
+#include "demag_yz.hpp"
 #include "newell_host.hpp"
 #include "stages.cuh"
 
@@ -211,6 +212,7 @@ struct Impl {
                 }
             }
         });
+        if (ok && !b.thin && b.want_yz && !yz_configure<T>(b)) return false;
         return ok;
     }
 
@@ -233,6 +235,9 @@ struct Impl {
                     k_yc_r<T, L1, L2><<<(b.nkx + b.kb_y - 1) / b.kb_y, b.thr_yc, b.rsm_yc, b.stream>>>(a);
                 }
             });
+        } else if (b.use_yz) {
+            ProfScope p(b, "demag_yz");
+            if (!yz_launch(b, a)) return false;
         } else {
             const long long lines = 3LL * b.nz * b.nkx;
             const unsigned gy = (unsigned)((lines + b.lines_y - 1) / b.lines_y);
@@ -337,6 +342,9 @@ struct Impl {
         if (b.thin) {
             ProfScope p(b, "demag_y_conv");
             k_y_conv<T><<<(b.nkx + b.kb_y - 1) / b.kb_y, 256, b.smem_yc, b.stream>>>(a);
+        } else if (b.use_yz) {
+            ProfScope p(b, "demag_yz");
+            if (!yz_launch(b, a)) return false;
         } else {
             const long long lines = 3LL * b.nz * b.nkx;
             const unsigned gy = (unsigned)((lines + b.lines_y - 1) / b.lines_y);
@@ -396,6 +404,19 @@ struct Impl {
         return dim3((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
     }
 
+    // One stage launch: the z-marching kernel for a uniform material, the
+    // general one (mask, Ms map, region LUT) otherwise.
+    template <int MODE>
+    static void launch_stage(Backend &b, const StageArgs<T> &s) {
+        if (b.stage_plain) {
+            const dim3 g((b.nx + 31) / 32, (b.ny + kStagePlainBY - 1) / kStagePlainBY,
+                         (b.nz + b.stage_zb - 1) / b.stage_zb);
+            k_stage_plain<T, MODE><<<g, dim3(32, kStagePlainBY, 1), 0, b.stream>>>(s, b.stage_zb);
+        } else {
+            k_stage<T, MODE><<<stage_grid(b), dim3(32, 4, 2), 0, b.stream>>>(s);
+        }
+    }
+
     // k = RHS(m, t); optional observables and diagnostics.
     static bool eval(Backend &b, const void *m, double t, void *kout, bool diag, bool obs) {
         StageArgs<T> s = stage_args(b, m, t);
@@ -407,7 +428,7 @@ struct Impl {
         s.out = b.d_out;
         {
             ProfScope p(b, "stage_eval");
-            k_stage<T, MODE_EVAL><<<stage_grid(b), dim3(32, 4, 2), 0, b.stream>>>(s);
+            launch_stage<MODE_EVAL>(b, s);
         }
         return check_launch(b, "stage_eval");
     }
@@ -474,7 +495,7 @@ struct Impl {
         s.half_dt = 0.5 * dt;
         {
             ProfScope p(b, "stage_heun_corr");
-            k_stage<T, MODE_HEUN_CORR><<<stage_grid(b), dim3(32, 4, 2), 0, b.stream>>>(s);
+            launch_stage<MODE_HEUN_CORR>(b, s);
         }
         if (!check_launch(b, "heun corrector")) return false;
         // fields, RHS (next k1) and diagnostics at the new state
@@ -532,7 +553,7 @@ struct Impl {
             s.dt = dt;
             {
                 ProfScope p(b, "stage_dp45_last");
-                k_stage<T, MODE_DP45_LAST><<<stage_grid(b), dim3(32, 4, 2), 0, b.stream>>>(s);
+                launch_stage<MODE_DP45_LAST>(b, s);
             }
             if (!check_launch(b, "dp45 last stage") || !read_stats(b)) return false;
             const double err = std::sqrt(b.h_out[Q_ERR2]);
@@ -670,7 +691,20 @@ bool backend_alloc(Backend &b) {
         items.push_back({(void **)&b.d_lut, (size_t)256 * 256 * 8});
     }
     if (b.has_ms_map) items.push_back({(void **)&b.d_msmap, (size_t)b.n * 8});
-    b.red_blocks = ((b.nx + 31) / 32) * ((b.ny + 3) / 4) * ((b.nz + 1) / 2);  // stage grid blocks
+    // stage kernels: the z-marching kernel serves a uniform material whose
+    // 3 n fits 32-bit indices; its planes per thread (zb) are halved until the
+    // grid has about 8 blocks per SM
+    b.stage_plain = !b.has_mask && !b.has_ms_map && !b.has_regions && 3ULL * (unsigned long long)b.n < (1ULL << 32);
+    {
+        auto blocks = [&](int zb) {
+            return (long long)((b.nx + 31) / 32) * ((b.ny + kStagePlainBY - 1) / kStagePlainBY) * ((b.nz + zb - 1) / zb);
+        };
+        int zb = std::max(1, b.nz);
+        while (zb > 1 && blocks(zb) < 148LL * 8) zb = (zb + 1) / 2;
+        b.stage_zb = zb;
+        const long long general = (long long)((b.nx + 31) / 32) * ((b.ny + 3) / 4) * ((b.nz + 1) / 2);
+        b.red_blocks = (int)std::max(general, blocks(zb));  // partials of either stage grid
+    }
     items.push_back({(void **)&b.partials, (size_t)NQ * b.red_blocks * 8});
     items.push_back({(void **)&b.d_out, (size_t)NQ * 8 + 64});
     items.push_back({(void **)&b.counter, 64});

@@ -67,6 +67,13 @@ struct Backend {
     bool use_reg = false;
     bool force_stockham = false;  // FULLMAG_FDM_FFT=stockham selects the shared-memory FFT
     int thr_x = 0, thr_y = 0, thr_yc = 0;
+    bool stage_plain = false;     // uniform material: z-marching stage kernel
+    int stage_zb = 1;             // z planes per thread of that kernel
+    bool use_yz = false;          // fused y-z cluster pass (3-D, register FFT)
+    bool want_yz = false;         // FULLMAG_FDM_YZ=fused selects it (default: three y/z kernels)
+    int yz_P = 0, thr_yz = 0;     // cluster size (ky residues per kx), threads
+    int yz_min_P = 1;             // FULLMAG_FDM_YZ_P: smallest cluster size tried
+    size_t rsm_yz = 0;
     size_t rsm_x = 0, rsm_y = 0, rsm_yc = 0;
 
     // ---- reductions ----

@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
     C *region = tw + L;
     const int LP = a.lines_x, RB = 2 * LP;
     const int c = blockIdx.z, z = blockIdx.y, y0 = blockIdx.x * RB;
-    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twx[k];
+    fill_tw4<L1, L2>(tw, a.twx, 1);
     __syncthreads();
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;
     const T *mc = a.m + (long long)c * a.n;
@@ -91,14 +91,11 @@ __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
     C *region = tw + L;
     const int LP = a.lines_x, RB = 2 * LP, nx = a.nx, ny = a.ny, nkx = a.nkx;
     const int c = blockIdx.z, z = blockIdx.y, y0 = blockIdx.x * RB;
-    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twx[k];
+    fill_tw4<L1, L2>(tw, a.twx, 1);
     // Z[k] = A[k] + i B[k] (k <= nx), Z[L-k] = conj(A[k]) + i conj(B[k]); DC and
     // Nyquist taken as real.  Row pairs (A, B) sit in adjacent lanes.
     const C *s1row = a.s1 + ((long long)c * a.nz + z) * nkx * ny;
-    auto gather = [&](int k, int r, bool ok) {
-        const int y = y0 + r;
-        C v = mk<T>(0, 0);
-        if (ok && y < ny) v = s1row[(long long)k * ny + y];
+    auto place = [&](int k, int r, bool ok, C v) {
         const T bx = __shfl_down_sync(0xffffffffu, v.x, 1);
         const T by = __shfl_down_sync(0xffffffffu, v.y, 1);
         if (ok && (r & 1) == 0) {
@@ -113,17 +110,36 @@ __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
         }
     };
     if (blockDim.x % RB == 0) {
-        // fixed row per thread, warp-uniform trip count (the shuffle needs whole warps)
+        // fixed row per thread, warp-uniform trip count (the shuffle needs whole
+        // warps); U independent loads in flight per thread before they are placed
+        constexpr int U = 8;
         const int r = threadIdx.x % RB, kstep = blockDim.x / RB, k0 = threadIdx.x / RB;
+        const int y = y0 + r;
         const int iters = (nkx + kstep - 1) / kstep;
-        for (int it = 0; it < iters; ++it) {
-            const int k = k0 + it * kstep;
-            gather(k < nkx ? k : 0, r, k < nkx);
+        for (int it0 = 0; it0 < iters; it0 += U) {
+            C vv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k = k0 + (it0 + u) * kstep;
+                vv[u] = (k < nkx && y < ny) ? s1row[(long long)k * ny + y] : mk<T>(0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (it0 + u < iters) {
+                    const int k = k0 + (it0 + u) * kstep;
+                    place(k < nkx ? k : 0, r, k < nkx, vv[u]);
+                }
+            }
         }
     } else {
         const int total = nkx * RB;
         const int span = (total + 31) / 32 * 32;
-        for (int u = threadIdx.x; u < span; u += blockDim.x) gather(u / RB, u % RB, u < total);
+        for (int u = threadIdx.x; u < span; u += blockDim.x) {
+            const int k = u / RB, r = u % RB, y = y0 + r;
+            const bool ok = u < total;
+            const C v = (ok && y < ny) ? s1row[(long long)k * ny + y] : mk<T>(0, 0);
+            place(k, r, ok, v);
+        }
     }
     __syncthreads();
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;
@@ -152,7 +168,7 @@ __global__ void __launch_bounds__(256) k_yf_r(DemagArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *region = tw + L;
-    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twy[k];
+    fill_tw4<L1, L2>(tw, a.twy, 1);
     __syncthreads();
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2, ny = a.ny;
     const long long total = 3LL * a.nz * a.nkx;
@@ -173,7 +189,7 @@ __global__ void __launch_bounds__(256) k_yi_r(DemagArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *region = tw + L;
-    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twy[k];
+    fill_tw4<L1, L2>(tw, a.twy, 1);
     __syncthreads();
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2, ny = a.ny;
     const long long total = 3LL * a.nz * a.nkx;
@@ -291,7 +307,7 @@ __global__ void __launch_bounds__(256) k_yc_r(DemagArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *region = tw + L;
-    for (int k = threadIdx.x; k < L; k += blockDim.x) tw[k] = a.twy[k];
+    fill_tw4<L1, L2>(tw, a.twy, 1);
     __syncthreads();
     const int KB = a.kb_y, ny = a.ny, nkx = a.nkx;
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;

@@ -101,10 +101,22 @@ __host__ __device__ constexpr int l2_for(int L) {
 // Shared-memory tile (complex elements) one line needs for its transpose.
 __host__ __device__ constexpr int tile_elems(int L1, int L2) { return L2 == 1 ? 0 : L1 * (L2 + 1); }
 
+// The inter-level twiddles W_L^{t k1} in the order fft4step reads them,
+// twT[k1 L2 + t]: the L2 threads of a line read consecutive words for each k1,
+// where a plain W_L^k table read at t k1 puts the threads 2 t k1 banks apart
+// (up to 16-way conflicts).  g[k] = W_{L stride}^k, so g[stride k] = W_L^k.
+template <int L1, int L2, typename C>
+__device__ __forceinline__ void fill_tw4(C *twT, const C *__restrict__ g, int stride) {
+    for (int idx = threadIdx.x; idx < L1 * L2; idx += blockDim.x) {
+        const int k1 = idx / L2, t = idx - k1 * L2;
+        twT[idx] = g[stride * k1 * t];
+    }
+}
+
 // One line, L2 threads; t = thread index within the line group.
 //   in(j)        -> C   for j = t + L2 * i
 //   out(k, v)           for k = k1 + L1 * k2 (this thread's k1 = t + L2 * r)
-// tw: table of exp(-2 pi i k / L), k < L (shared or global); tile: this line's
+// tw: the table of fill_tw4 (shared memory); tile: this line's
 // scratch (tile_elems); ALIAS_IN: the inputs live in memory the tile overlaps
 // (barrier before the tile is written); ALIAS_OUT: out() writes memory the
 // tile overlaps (barrier before the outputs are written).  All threads of the
@@ -133,7 +145,7 @@ __device__ __forceinline__ void fft4step(int t, const C *__restrict__ tw, C *til
         for (int k1 = 0; k1 < L1; ++k1) {
             C x = v[brev<L1>(k1)];
             if (k1 != 0 && t != 0) {
-                const C w = tw[t * k1];
+                const C w = tw[k1 * L2 + t];
                 x = INV ? cmulc(x, w) : cmul(x, w);
             }
             tile[k1 * (L2 + 1) + t] = x;

@@ -312,6 +312,179 @@ __global__ void __launch_bounds__(256, 3) k_stage(StageArgs<T> a) {
     if (a.partials) block_reduce_final(acc, a.partials, a.counter, a.out);
 }
 
+// ---------------------------------------------------------------------------
+// Uniform material (no mask, no Ms map, no region LUT): the same per-cell
+// arithmetic as k_stage, organised for instruction economy.  block
+// (32, BY, 1): lane = x, threadIdx.y = y; each thread marches over the planes
+// z in [z0, z0 + zb), keeping m at z-1, z, z+1 in registers, takes the x
+// neighbours from the adjacent lanes by shuffles (the warp's edge lanes load
+// theirs), loads the y neighbours (rows the adjacent warps also load) and the
+// next plane's values one plane ahead, reuses the loaded neighbours for the
+// forward-pair exchange energy, and reduces the diagnostics once per block.
+// 32-bit cell indices (3 n < 2^32 is checked by the host).  Threads of cells
+// outside the grid load the clamped edge cell and neither store nor
+// accumulate, so every lane takes part in the shuffles.
+// ---------------------------------------------------------------------------
+constexpr int kStagePlainBY = 4;  // rows (warps) per block of k_stage_plain
+
+template <typename T>
+struct PlaneLoads {
+    T up[3];   // m(x, y, z + 1)
+    T yp[3];   // m(x, y + 1, z)
+    T ym[3];   // m(x, y - 1, z)
+    T hd[3];   // H_d(x, y, z)
+};
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(128, 4) k_stage_plain(StageArgs<T> a, int zb) {
+    using R = double;
+    double acc[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const unsigned n = (unsigned)a.n, sxy = (unsigned)nx * (unsigned)ny;
+    const int lane = threadIdx.x;
+    const int x = blockIdx.x * 32 + lane, y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z0 = blockIdx.z * zb, z1 = min(z0 + zb, nz);
+    const bool inxy = x < nx && y < ny;
+    const int xc = min(x, nx - 1), yc = min(y, ny - 1);
+    const T *f0 = a.m, *f1 = a.m + n, *f2 = a.m + 2 * (size_t)n;
+    const bool has_xp = x + 1 < nx, has_xm = x > 0, has_yp = yc + 1 < ny, has_ym = yc > 0;
+    const bool ex = a.enable_exchange, dm = a.enable_demag;
+    auto ld3 = [&](unsigned j, T (&v)[3]) { v[0] = f0[j]; v[1] = f1[j]; v[2] = f2[j]; };
+    auto load_plane = [&](int z, unsigned j, PlaneLoads<T> &L) {
+        if (z + 1 < nz) ld3(j + sxy, L.up); else { L.up[0] = f0[j]; L.up[1] = f1[j]; L.up[2] = f2[j]; }
+        if (ex) {
+            if (has_yp) ld3(j + nx, L.yp);
+            if (has_ym) ld3(j - nx, L.ym);
+        }
+        if (dm) { L.hd[0] = a.hd[j]; L.hd[1] = a.hd[n + j]; L.hd[2] = a.hd[2 * (size_t)n + j]; }
+        else { L.hd[0] = T(0); L.hd[1] = T(0); L.hd[2] = T(0); }
+    };
+    // cell-invariant values
+    const R ix2 = a.dinv[0], iy2 = a.dinv[1], iz2 = a.dinv[2];
+    const R pref = a.ex_pref;
+    const double sinv = (a.ac_omega != 0.0) ? sin(a.t * a.ac_omega) : 0.0;
+    const R hx0 = a.has_ext ? a.hext[0] + a.hac[0] * sinv : 0.0;
+    const R hx1 = a.has_ext ? a.hext[1] + a.hac[1] * sinv : 0.0;
+    const R hx2 = a.has_ext ? a.hext[2] + a.hac[2] * sinv : 0.0;
+    const R al = a.alpha, gb = -a.gamma_bar;
+    const R pr = a.precession ? 1.0 : 0.0;
+    const double coef = a.ms * a.vol * kMu0;
+    const double pair = a.aex * a.vol;
+
+    unsigned i = ((unsigned)z0 * (unsigned)ny + (unsigned)yc) * (unsigned)nx + (unsigned)xc;
+    T cT[3];
+    ld3(i, cT);
+    R c[3] = {(R)cT[0], (R)cT[1], (R)cT[2]};
+    R dn[3] = {c[0], c[1], c[2]};
+    if (z0 > 0) { T t3[3]; ld3(i - sxy, t3); dn[0] = t3[0]; dn[1] = t3[1]; dn[2] = t3[2]; }
+    PlaneLoads<T> L;
+    load_plane(z0, i, L);
+    for (int z = z0; z < z1; ++z, i += sxy) {
+        PlaneLoads<T> Ln;
+        if (z + 1 < z1) load_plane(z + 1, i + sxy, Ln);
+        // x neighbours: adjacent lanes; the warp's edge lanes load theirs
+        T xpT[3], xmT[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            xpT[k] = __shfl_down_sync(0xffffffffu, cT[k], 1);
+            xmT[k] = __shfl_up_sync(0xffffffffu, cT[k], 1);
+        }
+        if (!has_xp) { xpT[0] = cT[0]; xpT[1] = cT[1]; xpT[2] = cT[2]; }
+        else if (lane == 31) ld3(i + 1, xpT);
+        if (!has_xm) { xmT[0] = cT[0]; xmT[1] = cT[1]; xmT[2] = cT[2]; }
+        else if (lane == 0) ld3(i - 1, xmT);
+        R up[3] = {(R)L.up[0], (R)L.up[1], (R)L.up[2]};
+        if (z + 1 >= nz) { up[0] = c[0]; up[1] = c[1]; up[2] = c[2]; }
+        R h[3] = {0.0, 0.0, 0.0};
+        R yp[3], xp[3];
+        if (ex) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                xp[k] = (R)xpT[k];
+                yp[k] = has_yp ? (R)L.yp[k] : c[k];
+                const R ym = has_ym ? (R)L.ym[k] : c[k];
+                const R lap = (xp[k] - 2.0 * c[k] + (R)xmT[k]) * ix2 + (yp[k] - 2.0 * c[k] + ym) * iy2 +
+                              (up[k] - 2.0 * c[k] + dn[k]) * iz2;
+                h[k] = lap * pref;
+            }
+        }
+        const R d0 = L.hd[0], d1 = L.hd[1], d2 = L.hd[2];
+        const R e0 = (h[0] + d0) + hx0, e1 = (h[1] + d1) + hx1, e2 = (h[2] + d2) + hx2;
+        const R cx_ = c[0], cy_ = c[1], cz_ = c[2];
+        const R p0 = cy_ * e2 - cz_ * e1, p1 = cz_ * e0 - cx_ * e2, p2 = cx_ * e1 - cy_ * e0;
+        const R q0 = cy_ * p2 - cz_ * p1, q1 = cz_ * p0 - cx_ * p2, q2 = cx_ * p1 - cy_ * p0;
+        const R r0 = (pr * p0 + q0 * al) * gb, r1 = (pr * p1 + q1 * al) * gb, r2 = (pr * p2 + q2 * al) * gb;
+        if (inxy) {
+            if (a.kout) { a.kout[i] = (T)r0; a.kout[n + i] = (T)r1; a.kout[2 * (size_t)n + i] = (T)r2; }
+            if (a.hex_out) { a.hex_out[i] = (T)h[0]; a.hex_out[n + i] = (T)h[1]; a.hex_out[2 * (size_t)n + i] = (T)h[2]; }
+            if (a.heff_out) { a.heff_out[i] = (T)e0; a.heff_out[n + i] = (T)e1; a.heff_out[2 * (size_t)n + i] = (T)e2; }
+            if (MODE == MODE_HEUN_CORR) {
+                const double hd_ = a.half_dt;
+                const double v0 = (double)a.m0[i] + ((double)a.k1[i] + r0) * hd_;
+                const double v1 = (double)a.m0[n + i] + ((double)a.k1[n + i] + r1) * hd_;
+                const double v2 = (double)a.m0[2 * (size_t)n + i] + ((double)a.k1[2 * (size_t)n + i] + r2) * hd_;
+                const double n2 = v0 * v0 + v1 * v1 + v2 * v2;
+                double inv;
+                if (sizeof(T) == 8) {
+                    const double nn = sqrt(n2);
+                    inv = nn > 0.0 ? 1.0 / nn : 0.0;
+                } else {
+                    inv = n2 > 0.0 ? rsqrt(n2) : 0.0;
+                }
+                a.m0[i] = (T)(v0 * inv); a.m0[n + i] = (T)(v1 * inv); a.m0[2 * (size_t)n + i] = (T)(v2 * inv);
+            }
+            if (a.partials) {
+                if (MODE == MODE_DP45_LAST) {
+                    const double E[6] = {71.0 / 57600.0, -71.0 / 16695.0, 71.0 / 1920.0,
+                                         -17253.0 / 339200.0, 22.0 / 525.0, -1.0 / 40.0};
+                    const double rr[3] = {(double)(T)r0, (double)(T)r1, (double)(T)r2};
+                    double er[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        double e = 0.0;
+#pragma unroll
+                        for (int st = 0; st < 5; ++st) e += E[st] * (double)a.ke[st][k * (size_t)n + i];
+                        e += E[5] * rr[k];
+                        er[k] = e * a.dt;
+                    }
+                    acc[Q_ERR2] = fmax(acc[Q_ERR2], er[0] * er[0] + er[1] * er[1] + er[2] * er[2]);
+                }
+                if (ex) {
+                    // forward pairs (x+1, y+1, z+1) inside the grid, from the loaded neighbours
+                    if (has_xp) {
+                        const double ddx = xp[0] - cx_, ddy = xp[1] - cy_, ddz = xp[2] - cz_;
+                        acc[Q_EEX] += pair * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[0];
+                    }
+                    if (has_yp) {
+                        const double ddx = yp[0] - cx_, ddy = yp[1] - cy_, ddz = yp[2] - cz_;
+                        acc[Q_EEX] += pair * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[1];
+                    }
+                    if (z + 1 < nz) {
+                        const double ddx = up[0] - cx_, ddy = up[1] - cy_, ddz = up[2] - cz_;
+                        acc[Q_EEX] += pair * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[2];
+                    }
+                }
+                acc[Q_EDEMAG] += -0.5 * coef * (cx_ * d0 + cy_ * d1 + cz_ * d2);
+                acc[Q_EEXT] += -coef * (cx_ * hx0 + cy_ * hx1 + cz_ * hx2);
+                acc[Q_HEFF2] = fmax(acc[Q_HEFF2], e0 * e0 + e1 * e1 + e2 * e2);
+                acc[Q_HD2] = fmax(acc[Q_HD2], d0 * d0 + d1 * d1 + d2 * d2);
+                acc[Q_RHS2] = fmax(acc[Q_RHS2], r0 * r0 + r1 * r1 + r2 * r2);
+            }
+        }
+        // advance one plane
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            dn[k] = c[k];
+            cT[k] = (z + 1 < nz) ? L.up[k] : cT[k];
+            c[k] = (R)cT[k];
+        }
+        L = Ln;
+    }
+    if (a.partials) block_reduce_final(acc, a.partials, a.counter, a.out);
+}
+
 // m_out = normalize(m0 + sum_j c_j k_j) in the reference's per-stage order.
 // `form` selects the grouping used by crates/fullmag-engine/src/lib.rs:1418-1520:
 //   0: m0 + k1*(c0)                     (Heun predictor: c0 = dt; DP45 stage 2: A21*dt)

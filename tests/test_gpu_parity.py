@@ -340,17 +340,23 @@ def test_runtime_errors_are_reported():
     assert lib.fullmag_fdm_backend_last_error(be.handle) == b"out_len mismatch"
 
 
-@pytest.mark.parametrize("fft", ["register", "stockham"])
+@pytest.mark.parametrize("fft", ["register", "fused", "stockham"])
 @pytest.mark.parametrize("cells,prec", [((64, 16, 1), nf.PRECISION_DOUBLE), ((32, 16, 8), nf.PRECISION_DOUBLE),
                                         ((32, 16, 8), nf.PRECISION_SINGLE), ((64, 32, 16), nf.PRECISION_SINGLE),
                                         ((256, 64, 1), nf.PRECISION_DOUBLE)])
 def test_both_fft_paths_match_oracle(monkeypatch, fft, cells, prec):
-    """The register-FFT kernels (power-of-two lengths) and the shared-memory
-    Stockham kernels (any 2,3,5,7-smooth length; forced by FULLMAG_FDM_FFT)."""
+    """The register-FFT kernels (power-of-two lengths; the y-z convolution as
+    three kernels, or fused per kx plane with FULLMAG_FDM_YZ=fused) and the
+    shared-memory Stockham kernels (any 2,3,5,7-smooth length; forced by
+    FULLMAG_FDM_FFT)."""
     if fft == "stockham":
         monkeypatch.setenv("FULLMAG_FDM_FFT", "stockham")
     else:
         monkeypatch.delenv("FULLMAG_FDM_FFT", raising=False)
+    if fft == "fused":
+        monkeypatch.setenv("FULLMAG_FDM_YZ", "fused")
+    else:
+        monkeypatch.delenv("FULLMAG_FDM_YZ", raising=False)
     be, sim, _ = make_pair(cells, (2e-9, 2e-9, 2e-9), alpha=0.3, h_ext=(1e4, 0, 2e4), precision=prec,
                            symmetric_kernel=True, seed=7)
     err = _field_errors(be, sim.observe())
@@ -361,3 +367,27 @@ def test_both_fft_paths_match_oracle(monkeypatch, fft, cells, prec):
         be.step(2e-14)
         sim.step(2e-14)
     assert max_abs(be.copy_m(), sim.m) <= (1e-12 if prec == nf.PRECISION_DOUBLE else 1e-6)
+
+
+# (cells, precision): the fused y-z pass picks the smallest cluster of P CTAs per
+# kx plane whose 3 nz x (Ly / P) slab fits two CTAs per SM, so these grids run
+# it with P = 2 (FP32, FP64), P = 4 (FP64, one fold of the input line) and
+# P = 8 (FP32, three folds; the second also with Lz = 32, z split in pairs).
+# FP64 never needs P = 8: its register path stops at Ly = 1024, Lz = 16.
+@pytest.mark.parametrize("cells,prec", [((16, 512, 8), nf.PRECISION_SINGLE), ((16, 256, 8), nf.PRECISION_DOUBLE),
+                                        ((16, 512, 8), nf.PRECISION_DOUBLE), ((8, 2048, 8), nf.PRECISION_SINGLE),
+                                        ((8, 1024, 16), nf.PRECISION_SINGLE)])
+def test_fused_yz_cluster_pass_matches_oracle(monkeypatch, cells, prec):
+    monkeypatch.delenv("FULLMAG_FDM_FFT", raising=False)
+    monkeypatch.setenv("FULLMAG_FDM_YZ", "fused")
+    be, sim, _ = make_pair(cells, (2e-9, 2.5e-9, 3e-9), alpha=0.3, h_ext=(1e4, -5e3, 2e4), precision=prec,
+                           symmetric_kernel=True, seed=11)
+    be.set_profiling(True)
+    be.refresh_observables()
+    names = set(be.profile())
+    assert "demag_yz" in names and "demag_z_conv" not in names, names
+    err = _field_errors(be, sim.observe())
+    print(cells, prec, {k: f"{v:.2e}" for k, v in err.items()})
+    tol = 1e-13 if prec == nf.PRECISION_DOUBLE else 2e-6
+    for k, v in err.items():
+        assert v <= tol, (k, v)
