@@ -331,7 +331,11 @@ def run_ours(args):
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
                          "algorithmic_bytes_per_launch": dom_bytes, "traffic": traffic},
             "step_roofline": {"algorithmic_bytes_per_step": step_bytes,
-                              "achieved_gbs": step_bytes / (results["fp32"]["ms"] / K * 1e-3) / 1e9},
+                              "achieved_gbs": step_bytes / (results["fp32"]["ms"] / K * 1e-3) / 1e9,
+                              # per cell-update model B_Heun = 2 (78 s + 6 s_k) + 27 s, s = s_k = 4
+                              "model_bytes_per_cell_update": 2 * (78 * s32 + 6 * s32) + 27 * s32,
+                              "model_achieved_gbs": (2 * (78 * s32 + 6 * s32) + 27 * s32) * (v32 / world) / 1e9,
+                              "model_frac": (2 * (78 * s32 + 6 * s32) + 27 * s32) * (v32 / world) / 1e9 / peak},
             "kernels": kernels,
             "gpu_launches": launches,
             "device_bytes": results["fp32"]["mem"],

@@ -384,6 +384,12 @@ __global__ void __launch_bounds__(128, 4) k_stage_plain(StageArgs<T> a, int zb) 
     for (int z = z0; z < z1; ++z, i += sxy) {
         PlaneLoads<T> Ln;
         if (z + 1 < z1) load_plane(z + 1, i + sxy, Ln);
+        // the corrector's m0 and k1 of this cell, issued before the arithmetic
+        T m0v[3], k1v[3];
+        if (MODE == MODE_HEUN_CORR && inxy) {
+            m0v[0] = a.m0[i]; m0v[1] = a.m0[n + i]; m0v[2] = a.m0[2 * (size_t)n + i];
+            k1v[0] = a.k1[i]; k1v[1] = a.k1[n + i]; k1v[2] = a.k1[2 * (size_t)n + i];
+        }
         // x neighbours: adjacent lanes; the warp's edge lanes load theirs
         T xpT[3], xmT[3];
 #pragma unroll
@@ -422,9 +428,9 @@ __global__ void __launch_bounds__(128, 4) k_stage_plain(StageArgs<T> a, int zb) 
             if (a.heff_out) { a.heff_out[i] = (T)e0; a.heff_out[n + i] = (T)e1; a.heff_out[2 * (size_t)n + i] = (T)e2; }
             if (MODE == MODE_HEUN_CORR) {
                 const double hd_ = a.half_dt;
-                const double v0 = (double)a.m0[i] + ((double)a.k1[i] + r0) * hd_;
-                const double v1 = (double)a.m0[n + i] + ((double)a.k1[n + i] + r1) * hd_;
-                const double v2 = (double)a.m0[2 * (size_t)n + i] + ((double)a.k1[2 * (size_t)n + i] + r2) * hd_;
+                const double v0 = (double)m0v[0] + ((double)k1v[0] + r0) * hd_;
+                const double v1 = (double)m0v[1] + ((double)k1v[1] + r1) * hd_;
+                const double v2 = (double)m0v[2] + ((double)k1v[2] + r2) * hd_;
                 const double n2 = v0 * v0 + v1 * v1 + v2 * v2;
                 double inv;
                 if (sizeof(T) == 8) {
