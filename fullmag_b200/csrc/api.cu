@@ -9,8 +9,8 @@
 //   - length mismatches give FULLMAG_FDM_ERR_INVALID and a message;
 //   - last_error(NULL) is "null handle".
 // Additional validation (reported through last_error, never silently
-// accepted): non-positive cell sizes or Ms, region ids >= 256, integrators
-// or boundary tiers this library does not implement, spectra that are not
+// accepted): non-positive cell sizes or Ms, region ids >= 256, unknown
+// integrators, boundary tiers this library does not implement, spectra that are not
 // the real, even/odd Newell form, padded FFT lengths with prime factors > 7.
 #include <algorithm>
 #include <chrono>
@@ -193,9 +193,8 @@ bool create_impl(Backend &b, const fullmag_fdm_plan_desc *plan, const fullmag_fd
     if (b.precision != FULLMAG_FDM_PRECISION_SINGLE && b.precision != FULLMAG_FDM_PRECISION_DOUBLE) {
         b.last_error = "unknown precision"; return false;
     }
-    if (b.integrator != FULLMAG_FDM_INTEGRATOR_HEUN && b.integrator != FULLMAG_FDM_INTEGRATOR_DP45) {
-        b.last_error = "integrator " + std::to_string((int)b.integrator) +
-                       " is not implemented by this backend (HEUN and DP45 are)";
+    if (b.integrator < FULLMAG_FDM_INTEGRATOR_HEUN || b.integrator > FULLMAG_FDM_INTEGRATOR_RK23) {
+        b.last_error = "unknown integrator " + std::to_string((int)b.integrator);
         return false;
     }
     const uint64_t expected = (uint64_t)b.n * 3;

@@ -548,12 +548,16 @@ struct Impl {
             s.partials = b.partials;
             s.counter = b.counter;
             s.out = b.d_out;
+            // err = dt (E1 k1 + E3 k3 + E4 k4 + E5 k5 + E6 k6 + E7 k7), lib.rs:1653-1674
             s.ke[0] = (const T *)k[0]; s.ke[1] = (const T *)k[2]; s.ke[2] = (const T *)k[3];
             s.ke[3] = (const T *)k[4]; s.ke[4] = (const T *)k[5];
+            s.nke = 5;
+            s.ew[0] = 71.0 / 57600.0; s.ew[1] = -71.0 / 16695.0; s.ew[2] = 71.0 / 1920.0;
+            s.ew[3] = -17253.0 / 339200.0; s.ew[4] = 22.0 / 525.0; s.ew[5] = -1.0 / 40.0;
             s.dt = dt;
             {
                 ProfScope p(b, "stage_dp45_last");
-                launch_stage<MODE_DP45_LAST>(b, s);
+                launch_stage<MODE_ERR_LAST>(b, s);
             }
             if (!check_launch(b, "dp45 last stage") || !read_stats(b)) return false;
             const double err = std::sqrt(b.h_out[Q_ERR2]);
@@ -574,6 +578,128 @@ struct Impl {
             dt = std::min(std::max(dt_new, b.dt_min), b.dt_max);
             // k[0] still equals RHS(m0, t): nothing to recompute for stage 1
         }
+    }
+
+    // Fields and RHS at the accepted state into k[0] (the next step's k1), with
+    // the step diagnostics; advances the step counter.
+    static bool finish_step(Backend &b, double dt, fullmag_fdm_step_stats *st, bool readback) {
+        if (!demag(b, b.m, b.hd)) return false;
+        if (!eval(b, b.m, b.time, b.k[0], true, false)) return false;
+        b.step_count += 1;
+        b.k1_valid = true;
+        b.obs_valid = false;
+        if (readback) {
+            if (!read_stats(b)) return false;
+            fill_stats(b, dt, st);
+            st->suggested_next_dt = 0.0;
+        }
+        return true;
+    }
+
+    // One classical RK4 step (lib.rs:1253-1297) with the cached k1; stage
+    // times t, t + dt/2, t + dt/2, t + dt.
+    static bool rk4(Backend &b, double dt, fullmag_fdm_step_stats *st, bool readback) {
+        if (!ensure_k1(b)) return false;
+        void **k = b.k;
+        const double t = b.time;
+        if (!combine(b, 0, b.m, {k[0]}, {0.5 * dt}, dt, b.mstage)) return false;
+        if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + 0.5 * dt, k[1], false, false)) return false;
+        if (!combine(b, 0, b.m, {k[1]}, {0.5 * dt}, dt, b.mstage)) return false;
+        if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + 0.5 * dt, k[2], false, false)) return false;
+        if (!combine(b, 0, b.m, {k[2]}, {dt}, dt, b.mstage)) return false;
+        if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + dt, k[3], false, false)) return false;
+        // m <- normalize(m0 + ((k1 + 2 k2) + (2 k3 + k4)) dt/6), in place
+        if (!combine(b, 3, b.m, {k[0], k[1], k[2], k[3]}, {1.0, 2.0, 2.0, 1.0}, dt / 6.0, b.m)) return false;
+        b.time += dt;
+        return finish_step(b, dt, st, readback);
+    }
+
+    // One accepted Bogacki-Shampine 2(3) step (lib.rs:1332-1407).  The
+    // reference evaluates k1 = RHS(m0) on every attempt; the cached k1 holds the
+    // same values.  Stage times t, t + dt/2, t + 3dt/4, t + dt; k4 = RHS(y3) is
+    // the next step's k1.
+    static bool rk23(Backend &b, double dt_in, fullmag_fdm_step_stats *st) {
+        double dt = std::max(std::min(dt_in, b.dt_max), b.dt_min);
+        if (!ensure_k1(b)) return false;
+        void **k = b.k;
+        for (;;) {
+            const double t = b.time;
+            if (!combine(b, 0, b.m, {k[0]}, {0.5 * dt}, dt, b.mstage)) return false;
+            if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + 0.5 * dt, k[1], false, false)) return false;
+            if (!combine(b, 0, b.m, {k[1]}, {0.75 * dt}, dt, b.mstage)) return false;
+            if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + 0.75 * dt, k[2], false, false)) return false;
+            if (!combine(b, 2, b.m, {k[0], k[1], k[2]}, {2.0 / 9.0, 1.0 / 3.0, 4.0 / 9.0}, dt, b.mstage)) return false;
+            if (!demag(b, b.mstage, b.hd)) return false;
+            StageArgs<T> s = stage_args(b, b.mstage, t + dt);
+            s.kout = (T *)k[3];
+            s.partials = b.partials;
+            s.counter = b.counter;
+            s.out = b.d_out;
+            s.ke[0] = (const T *)k[0]; s.ke[1] = (const T *)k[1]; s.ke[2] = (const T *)k[2];
+            s.nke = 3;
+            s.ew[0] = -5.0 / 72.0; s.ew[1] = 1.0 / 12.0; s.ew[2] = 1.0 / 9.0; s.ew[3] = -1.0 / 8.0;
+            s.dt = dt;
+            {
+                ProfScope p(b, "stage_rk23_last");
+                launch_stage<MODE_ERR_LAST>(b, s);
+            }
+            if (!check_launch(b, "rk23 last stage") || !read_stats(b)) return false;
+            const double err = std::sqrt(b.h_out[Q_ERR2]);
+            if (err <= b.max_error || dt <= b.dt_min) {
+                std::swap(b.m, b.mstage);
+                std::swap(k[0], k[3]);
+                b.time += dt;
+                b.step_count += 1;
+                b.k1_valid = true;
+                b.obs_valid = false;
+                fill_stats(b, dt, st);
+                st->suggested_next_dt = std::min(
+                    std::max(b.headroom * dt * std::pow(b.max_error / std::max(err, 1e-30), 1.0 / 3.0), b.dt_min),
+                    b.dt_max);
+                return true;
+            }
+            const double dt_new = b.headroom * dt * std::pow(b.max_error / err, 1.0 / 3.0);
+            dt = std::min(std::max(dt_new, b.dt_min), b.dt_max);
+        }
+    }
+
+    // ABM3 (lib.rs:1573-1648).  History f_n, f_{n-1}, f_{n-2} in k[2], k[3],
+    // k[4] (pointer rotation), k[1] the slot the next entry is written to.
+    // Three Heun start-up steps push RHS(m_{n+1}); then AB3 predictor,
+    // f* = RHS(predicted) at t + dt, AM3 corrector, push f*.  A dt more than 10 %
+    // away from the last one restarts the history before the step
+    // (native/backends/fdm/src/llg_abm3_fp64.cu:177-180).  The history survives
+    // magnetisation uploads, as in the reference.
+    static void abm_push(Backend &b, double dt) {
+        void **k = b.k;
+        void *spare = k[4];
+        k[4] = k[3];
+        k[3] = k[2];
+        k[2] = k[1];
+        k[1] = spare;
+        b.abm_startup = std::min(b.abm_startup + 1, 3);
+        b.abm_last_dt = dt;
+    }
+
+    static bool abm3(Backend &b, double dt, fullmag_fdm_step_stats *st, bool readback) {
+        if (b.abm_last_dt > 0.0 && std::fabs(dt - b.abm_last_dt) / b.abm_last_dt > 0.1) b.abm_startup = 0;
+        void **k = b.k;
+        if (b.abm_startup < 3) {
+            if (!heun(b, dt, st, readback)) return false;
+            // heun() left RHS(m_{n+1}) in k[0]; the history keeps a copy
+            if (!cuda_ok(b, cudaMemcpyAsync(k[1], k[0], (size_t)3 * b.n * sizeof(T), cudaMemcpyDeviceToDevice, b.stream),
+                         "abm history"))
+                return false;
+            abm_push(b, dt);
+            return true;
+        }
+        const double t = b.time;
+        if (!combine(b, 2, b.m, {k[2], k[3], k[4]}, {23.0 / 12.0, -16.0 / 12.0, 5.0 / 12.0}, dt, b.mstage)) return false;
+        if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + dt, k[1], false, false)) return false;
+        if (!combine(b, 2, b.m, {k[1], k[2], k[3]}, {5.0 / 12.0, 8.0 / 12.0, -1.0 / 12.0}, dt, b.m)) return false;
+        b.time += dt;
+        abm_push(b, dt);
+        return finish_step(b, dt, st, readback);
     }
 
     static bool refresh(Backend &b) {
@@ -669,7 +795,12 @@ bool backend_alloc(Backend &b) {
     // layout sizes
     struct Item { void **p; size_t bytes; };
     std::vector<Item> items;
-    const int nk = b.integrator == FULLMAG_FDM_INTEGRATOR_DP45 ? 7 : 2;
+    // k buffers: DP45 k1..k7; RK4 and RK23 k1..k4; ABM3 k1, the next history
+    // slot and f_n, f_{n-1}, f_{n-2}; Heun k1 (k2 stays in registers) + 1
+    const int nk = b.integrator == FULLMAG_FDM_INTEGRATOR_DP45   ? 7
+                   : b.integrator == FULLMAG_FDM_INTEGRATOR_ABM3 ? 5
+                   : (b.integrator == FULLMAG_FDM_INTEGRATOR_RK4 || b.integrator == FULLMAG_FDM_INTEGRATOR_RK23) ? 4
+                                                                   : 2;
     items.push_back({&b.m, vec});
     items.push_back({&b.mstage, vec});
     items.push_back({&b.hd, vec});
@@ -773,13 +904,26 @@ bool backend_refresh(Backend &b) {
     return b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::refresh(b) : Impl<float>::refresh(b);
 }
 
+// One step of the plan's integrator; `last` asks for the stats readback (the
+// adaptive integrators always read back: their error decides acceptance).
+template <typename T>
+static bool step_once(Backend &b, double dt, fullmag_fdm_step_stats *st, bool last) {
+    switch (b.integrator) {
+        case FULLMAG_FDM_INTEGRATOR_DP45: return Impl<T>::dp45(b, dt, st);
+        case FULLMAG_FDM_INTEGRATOR_RK23: return Impl<T>::rk23(b, dt, st);
+        case FULLMAG_FDM_INTEGRATOR_RK4: return Impl<T>::rk4(b, dt, st, last);
+        case FULLMAG_FDM_INTEGRATOR_ABM3: return Impl<T>::abm3(b, dt, st, last);
+        default: return Impl<T>::heun(b, dt, st, last);
+    }
+}
+
+static bool adaptive(const Backend &b) {
+    return b.integrator == FULLMAG_FDM_INTEGRATOR_DP45 || b.integrator == FULLMAG_FDM_INTEGRATOR_RK23;
+}
+
 bool backend_step(Backend &b, double dt, fullmag_fdm_step_stats *st) {
-    bool ok;
-    if (b.integrator == FULLMAG_FDM_INTEGRATOR_DP45)
-        ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::dp45(b, dt, st) : Impl<float>::dp45(b, dt, st);
-    else
-        ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::heun(b, dt, st, true)
-                                                         : Impl<float>::heun(b, dt, st, true);
+    const bool ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? step_once<double>(b, dt, st, true)
+                                                                : step_once<float>(b, dt, st, true);
     if (b.profiling) prof_collect(b);
     return ok;
 }
@@ -788,13 +932,9 @@ bool backend_step_n(Backend &b, double dt, uint32_t nsteps, fullmag_fdm_step_sta
     bool ok = true;
     for (uint32_t i = 0; i < nsteps && ok; ++i) {
         const bool last = (i + 1 == nsteps);
-        if (b.integrator == FULLMAG_FDM_INTEGRATOR_DP45) {
-            ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::dp45(b, dt, st) : Impl<float>::dp45(b, dt, st);
-            if (ok) dt = st->suggested_next_dt;
-        } else {
-            ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::heun(b, dt, st, last)
-                                                             : Impl<float>::heun(b, dt, st, last);
-        }
+        ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? step_once<double>(b, dt, st, last)
+                                                         : step_once<float>(b, dt, st, last);
+        if (ok && adaptive(b)) dt = st->suggested_next_dt;
     }
     if (b.profiling) prof_collect(b);
     return ok;

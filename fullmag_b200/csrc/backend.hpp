@@ -47,6 +47,8 @@ struct Backend {
     size_t scalar = 8;        // bytes per state scalar
     void *m = nullptr, *mstage = nullptr, *hd = nullptr;
     void *k[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    int abm_startup = 0;          // ABM3 start-up steps done (0..3)
+    double abm_last_dt = 0.0;     // dt of the last ABM3 step
     void *hex = nullptr, *heff = nullptr;
     void *staging = nullptr;  // device AoS staging (>= 3 n doubles)
     uint8_t *d_mask = nullptr;

@@ -36,7 +36,7 @@ __host__ __device__ constexpr bool q_is_max(int q) { return q >= Q_HEFF2; }
 enum : int {
     MODE_EVAL = 0,        // k = RHS(m); optional observables / diagnostics
     MODE_HEUN_CORR = 1,   // k2 = RHS(m_p); m <- normalize(m0 + dt/2 (k1 + k2))
-    MODE_DP45_LAST = 2,   // k7 = RHS(y); diagnostics + embedded error norm
+    MODE_ERR_LAST = 2,    // k_last = RHS(y); diagnostics + embedded error norm (DP45, RK23)
 };
 
 template <typename T>
@@ -70,8 +70,11 @@ struct StageArgs {
     T *m0;                          // in: m0; out: corrected m (same buffer)
     const T *k1;
     double half_dt;
-    // MODE_DP45_LAST: error weights on k1,k3,k4,k5,k6,k7
+    // MODE_ERR_LAST: err = dt (sum_j ew[j] ke[j] + ew[nke] k_last), accumulated
+    // from zero in that order (max_error_norm_buf, lib.rs:1653-1674)
     const T *ke[5];
+    double ew[6];
+    int nke;
     double dt;
 };
 
@@ -266,19 +269,15 @@ __global__ void __launch_bounds__(256, 3) k_stage(StageArgs<T> a) {
                 a.m0[i] = (T)(v0 * inv); a.m0[n + i] = (T)(v1 * inv); a.m0[2 * n + i] = (T)(v2 * inv);
             }
             if (a.partials) {
-                if (MODE == MODE_DP45_LAST) {
-                    // err = dt * (E1 k1 + E3 k3 + E4 k4 + E5 k5 + E6 k6 + E7 k7), lib.rs:1653-1674
-                    const double E[6] = {71.0 / 57600.0, -71.0 / 16695.0, 71.0 / 1920.0,
-                                         -17253.0 / 339200.0, 22.0 / 525.0, -1.0 / 40.0};
-                    // the stored k7 (rounded to T) enters the error like the other stages
+                if (MODE == MODE_ERR_LAST) {
+                    // the stored last stage (rounded to T) enters the error like the others
                     const double rr[3] = {(double)(T)r0, (double)(T)r1, (double)(T)r2};
                     double er[3];
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         double e = 0.0;
-#pragma unroll
-                        for (int st = 0; st < 5; ++st) e += E[st] * (double)a.ke[st][c * n + i];
-                        e += E[5] * rr[c];
+                        for (int st = 0; st < a.nke; ++st) e += a.ew[st] * (double)a.ke[st][c * n + i];
+                        e += a.ew[a.nke] * rr[c];
                         er[c] = e * a.dt;
                     }
                     acc[Q_ERR2] = fmax(acc[Q_ERR2], er[0] * er[0] + er[1] * er[1] + er[2] * er[2]);
@@ -442,17 +441,14 @@ __global__ void __launch_bounds__(128, 4) k_stage_plain(StageArgs<T> a, int zb) 
                 a.m0[i] = (T)(v0 * inv); a.m0[n + i] = (T)(v1 * inv); a.m0[2 * (size_t)n + i] = (T)(v2 * inv);
             }
             if (a.partials) {
-                if (MODE == MODE_DP45_LAST) {
-                    const double E[6] = {71.0 / 57600.0, -71.0 / 16695.0, 71.0 / 1920.0,
-                                         -17253.0 / 339200.0, 22.0 / 525.0, -1.0 / 40.0};
+                if (MODE == MODE_ERR_LAST) {
                     const double rr[3] = {(double)(T)r0, (double)(T)r1, (double)(T)r2};
                     double er[3];
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         double e = 0.0;
-#pragma unroll
-                        for (int st = 0; st < 5; ++st) e += E[st] * (double)a.ke[st][k * (size_t)n + i];
-                        e += E[5] * rr[k];
+                        for (int st = 0; st < a.nke; ++st) e += a.ew[st] * (double)a.ke[st][k * (size_t)n + i];
+                        e += a.ew[a.nke] * rr[k];
                         er[k] = e * a.dt;
                     }
                     acc[Q_ERR2] = fmax(acc[Q_ERR2], er[0] * er[0] + er[1] * er[1] + er[2] * er[2]);

@@ -385,6 +385,10 @@ struct Problem {
     double t = 0.0;
     bool fsal_valid = false;
     std::vector<V3> fsal;
+    // ABM3 history (AbmHistory, lib.rs:628-687): f_n, f_{n-1}, f_{n-2}
+    std::vector<V3> abm_fn, abm_fn1, abm_fn2;
+    int abm_startup = 0;
+    double abm_last_dt = 0.0;
     // FFT workspace (FftWorkspace, lib.rs:288-380)
     size_t px = 0, py = 0, pz = 0, plen = 0;
     FftPlan fwx, fwy, fwz, ivx, ivy, ivz;
@@ -662,6 +666,144 @@ struct Problem {
         r.suggested_next_dt = 0.0;
     }
 
+    // Stage state normalize(m0 + inc(i)) into ms.
+    template <class Inc>
+    void stage_state(const std::vector<V3> &m0, Inc inc, std::vector<V3> &ms) {
+#pragma omp parallel for
+        for (long il = 0; il < (long)n; ++il) {
+            size_t i = (size_t)il;
+            ms[i] = normalized(add(m0[i], inc(i)));
+        }
+    }
+
+    // rk4_step_buf (lib.rs:1253-1297); stage times t, t + dt/2, t + dt/2, t + dt
+    // for the time-dependent Zeeman extension.
+    void rk4(double dt, oracle_report &r) {
+        std::vector<V3> m0 = m, k1, k2, k3, k4, ms(n);
+        rhs_into(m0, t, k1);
+        stage_state(m0, [&](size_t i) { return scale(k1[i], 0.5 * dt); }, ms);
+        rhs_into(ms, t + 0.5 * dt, k2);
+        stage_state(m0, [&](size_t i) { return scale(k2[i], 0.5 * dt); }, ms);
+        rhs_into(ms, t + 0.5 * dt, k3);
+        stage_state(m0, [&](size_t i) { return scale(k3[i], dt); }, ms);
+        rhs_into(ms, t + dt, k4);
+        stage_state(m0, [&](size_t i) {
+            return scale(add(add(k1[i], scale(k2[i], 2.0)), add(scale(k3[i], 2.0), k4[i])), dt / 6.0);
+        }, m);
+        t += dt;
+        Fields F;
+        diagnostics(m, t, F, r);
+        r.time_seconds = t;
+        r.dt_used = dt;
+        r.suggested_next_dt = 0.0;
+    }
+
+    // max_error_norm_buf (lib.rs:1653-1674): max_i |dt sum_j w_j k_j[i]|, the
+    // sum accumulated from zero in the listed order.
+    double error_norm(std::initializer_list<std::pair<const std::vector<V3> *, double>> ws, double dt) {
+        double err = 0.0;
+#pragma omp parallel for reduction(max : err)
+        for (long il = 0; il < (long)n; ++il) {
+            size_t i = (size_t)il;
+            V3 e = {0, 0, 0};
+            for (auto &w : ws) {
+                e[0] += w.second * (*w.first)[i][0];
+                e[1] += w.second * (*w.first)[i][1];
+                e[2] += w.second * (*w.first)[i][2];
+            }
+            e[0] *= dt; e[1] *= dt; e[2] *= dt;
+            err = std::max(err, norm(e));
+        }
+        return err;
+    }
+
+    // rk23_step_buf (lib.rs:1332-1407), Bogacki-Shampine 2(3): k1 is evaluated
+    // at m0 on every attempt (the same values each time); stage times t,
+    // t + dt/2, t + 3dt/4, t + dt.
+    void rk23(double dt_in, oracle_report &r) {
+        double max_error = d.max_error > 0 ? d.max_error : 1e-5;
+        double dt_min = d.dt_min > 0 ? d.dt_min : 1e-18;
+        double dt_max = d.dt_max > 0 ? d.dt_max : 1e-10;
+        double headroom = d.headroom > 0 ? d.headroom : 0.8;
+        double dt = std::max(std::min(dt_in, dt_max), dt_min);
+        std::vector<V3> m0 = m, k1, k2, k3, k4, ms(n);
+        int rejected = 0;
+        for (;;) {
+            rhs_into(m0, t, k1);
+            stage_state(m0, [&](size_t i) { return scale(k1[i], 0.5 * dt); }, ms);
+            rhs_into(ms, t + 0.5 * dt, k2);
+            stage_state(m0, [&](size_t i) { return scale(k2[i], 0.75 * dt); }, ms);
+            rhs_into(ms, t + 0.75 * dt, k3);
+            stage_state(m0, [&](size_t i) {
+                return scale(add(add(scale(k1[i], 2.0 / 9.0), scale(k2[i], 1.0 / 3.0)), scale(k3[i], 4.0 / 9.0)), dt);
+            }, ms);
+            rhs_into(ms, t + dt, k4);
+            const double err = error_norm({{&k1, -5.0 / 72.0}, {&k2, 1.0 / 12.0}, {&k3, 1.0 / 9.0}, {&k4, -1.0 / 8.0}}, dt);
+            if (err <= max_error || dt <= dt_min) {
+                m = ms;
+                t += dt;
+                const double dt_next = std::min(
+                    std::max(headroom * dt * std::pow(max_error / std::max(err, 1e-30), 1.0 / 3.0), dt_min), dt_max);
+                Fields F;
+                diagnostics(m, t, F, r);
+                r.time_seconds = t;
+                r.dt_used = dt;
+                r.suggested_next_dt = dt_next;
+                r.rejected_attempts = rejected;
+                return;
+            }
+            ++rejected;
+            const double dt_new = headroom * dt * std::pow(max_error / err, 1.0 / 3.0);
+            dt = std::min(std::max(dt_new, dt_min), dt_max);
+        }
+    }
+
+    // abm3_step_buf (lib.rs:1573-1648): three Heun start-up steps push
+    // f(m_{n+1}); then AB3 predictor, f* = f(predicted), AM3 corrector, push f*.
+    // A dt that differs from the last one by more than 10 % restarts the
+    // history before the step, as the reference's CUDA backend does
+    // (native/backends/fdm/src/llg_abm3_fp64.cu:177-180); the CPU engine checks
+    // at the push after the step (lib.rs:672-676).  Both agree for constant dt.
+    void abm_push(std::vector<V3> f, double dt) {
+        abm_fn2 = std::move(abm_fn1);
+        abm_fn1 = std::move(abm_fn);
+        abm_fn = std::move(f);
+        abm_startup = std::min(abm_startup + 1, 3);
+        abm_last_dt = dt;
+    }
+
+    void abm3(double dt, oracle_report &r) {
+        if (abm_last_dt > 0.0 && std::fabs(dt - abm_last_dt) / abm_last_dt > 0.1) abm_startup = 0;
+        std::vector<V3> m0 = m, ms(n);
+        if (abm_startup < 3) {
+            std::vector<V3> k1, k2, fa;
+            rhs_into(m0, t, k1);
+            stage_state(m0, [&](size_t i) { return scale(k1[i], dt); }, ms);
+            rhs_into(ms, t + dt, k2);
+            stage_state(m0, [&](size_t i) { return scale(add(k1[i], k2[i]), 0.5 * dt); }, m);
+            t += dt;
+            rhs_into(m, t, fa);
+            abm_push(std::move(fa), dt);
+        } else {
+            const std::vector<V3> &fn = abm_fn, &fn1 = abm_fn1, &fn2 = abm_fn2;
+            std::vector<V3> fs;
+            stage_state(m0, [&](size_t i) {
+                return scale(add(add(scale(fn[i], 23.0 / 12.0), scale(fn1[i], -16.0 / 12.0)), scale(fn2[i], 5.0 / 12.0)), dt);
+            }, ms);
+            rhs_into(ms, t + dt, fs);
+            stage_state(m0, [&](size_t i) {
+                return scale(add(add(scale(fs[i], 5.0 / 12.0), scale(fn[i], 8.0 / 12.0)), scale(fn1[i], -1.0 / 12.0)), dt);
+            }, m);
+            t += dt;
+            abm_push(std::move(fs), dt);
+        }
+        Fields F;
+        diagnostics(m, t, F, r);
+        r.time_seconds = t;
+        r.dt_used = dt;
+        r.suggested_next_dt = 0.0;
+    }
+
     // rk45_step_buf (lib.rs:1412-1568) with max_error_norm_buf (lib.rs:1653-1674)
     void dp45(double dt_in, oracle_report &r) {
         double max_error = d.max_error > 0 ? d.max_error : 1e-5;
@@ -863,8 +1005,13 @@ void oracle_destroy(oracle_problem *p) { delete p; }
 int oracle_step(oracle_problem *op, double dt, oracle_report *out) {
     if (!op || !out || !(dt > 0.0)) return -1;
     std::memset(out, 0, sizeof(*out));
-    if (op->p.d.integrator == ORACLE_DP45) op->p.dp45(dt, *out);
-    else op->p.heun(dt, *out);
+    switch (op->p.d.integrator) {
+        case ORACLE_DP45: op->p.dp45(dt, *out); break;
+        case ORACLE_ABM3: op->p.abm3(dt, *out); break;
+        case ORACLE_RK4: op->p.rk4(dt, *out); break;
+        case ORACLE_RK23: op->p.rk23(dt, *out); break;
+        default: op->p.heun(dt, *out); break;
+    }
     return 0;
 }
 

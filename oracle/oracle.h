@@ -3,7 +3,7 @@
  *
  * The oracle is a C++ restatement of the reference's CPU engine for the
  * single-grid Exchange + Demag + Zeeman + LLG FDM path:
- *   crates/fullmag-engine/src/lib.rs        (fields, Heun, DP45, energies, FFT driver)
+ *   crates/fullmag-engine/src/lib.rs        (fields, Heun, DP45, RK4, RK23, ABM3, energies, FFT driver)
  *   crates/fullmag-engine/src/vector.rs     (normalisation and vector helpers)
  *   crates/fullmag-fdm-demag/src/newell.rs  (Newell tensor, real space)
  *   crates/fullmag-plan/src/lib.rs:1928-1957 (seeded random unit vectors)
@@ -31,16 +31,19 @@ extern "C" {
 
 typedef struct oracle_problem oracle_problem;
 
-enum {
+enum {  /* values of fullmag_fdm_integrator (native/include/fullmag_fdm.h:52-58) */
     ORACLE_HEUN = 1,
     ORACLE_DP45 = 2,
+    ORACLE_ABM3 = 3,
+    ORACLE_RK4 = 4,
+    ORACLE_RK23 = 5,
 };
 
 typedef struct {
     uint32_t nx, ny, nz;
     double dx, dy, dz;
     double ms, aex, alpha, gamma;
-    int integrator;           /* ORACLE_HEUN / ORACLE_DP45 */
+    int integrator;           /* ORACLE_HEUN / _DP45 / _ABM3 / _RK4 / _RK23 */
     int precession_enabled;   /* 0 = pure damping */
     int enable_exchange;
     int enable_demag;

@@ -21,6 +21,9 @@ _lib = None
 
 HEUN = 1
 DP45 = 2
+ABM3 = 3
+RK4 = 4
+RK23 = 5
 
 
 class OracleDesc(C.Structure):

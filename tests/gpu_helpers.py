@@ -42,7 +42,7 @@ def make_pair(cells, cell_size, ms=8e5, aex=1.3e-11, alpha=0.02, gamma=2.211e5, 
                       ac_field=ac_field, ac_frequency_hz=ac_freq, demag_source=demag_source)
     be = nf.NativeFdmBackend(plan)
     prob = O.Problem(nx, ny, nz, *cell_size, ms=ms, aex=aex, alpha=alpha, gamma=gamma,
-                     integrator=O.DP45 if integrator == nf.DP45 else O.HEUN,
+                     integrator=integrator,  # the oracle uses the ABI's integrator values
                      precession=not pure_damping, exchange=exchange, demag=demag, h_ext=h_ext,
                      active_mask=mask, region_mask=regions, exchange_lut=lut,
                      ms_map=ms_map, h_ac=ac_field, ac_freq=ac_freq,

@@ -93,7 +93,7 @@ def _bad_plan_error(**kw):
 
 def test_validation_errors_without_device():
     assert "initial_magnetization_len mismatch" in _bad_plan_error(initial_magnetization=np.zeros(9))
-    assert "not implemented" in _bad_plan_error(integrator=nf.RK4)
+    assert "unknown integrator" in _bad_plan_error(integrator=9)
     assert "active_mask_len mismatch" in _bad_plan_error(active_mask=np.ones(5))
     assert "region id" in _bad_plan_error(region_mask=np.full(24, 300))
     assert "cell sizes" in _bad_plan_error(cell_size=(0.0, 1e-9, 1e-9))

@@ -260,3 +260,105 @@ def test_dp45_controller_accepts_and_suggests():
     r = s.step(1e-13)
     assert r["dt_used"] <= 1e-13 and r["suggested_next_dt"] > 0
     assert abs(s.time - r["dt_used"]) < 1e-30
+
+
+# ---------------------------------------------------------------- RK4 / RK23 / ABM3
+# The reference has no known-answer tests for these integrators; the
+# restatement (lib.rs:1253-1407, 1573-1648) is pinned by its convergence
+# order on a smooth, non-chaotic problem, by the Heun start-up of ABM3 and by
+# the step controller of RK23.
+def _smooth_problem(integrator, **kw):
+    nx, ny, nz = 16, 8, 1
+    x = (np.arange(nx) + 0.5) / nx
+    m0 = np.zeros((nx * ny * nz, 3))
+    m0[:, 0] = np.tile(np.cos(0.6 * np.pi * x), ny)
+    m0[:, 1] = np.tile(np.sin(0.6 * np.pi * x), ny)
+    m0[:, 2] = 0.3
+    prob = O.Problem(nx, ny, nz, 3e-9, 3e-9, 3e-9, alpha=0.1, integrator=integrator,
+                     h_ext=(5e3, 2e4, -1e4), thin_film_2d=True, **kw)
+    return prob, m0.reshape(-1)
+
+
+def _final_m(integrator, dt, t_end, **kw):
+    prob, m0 = _smooth_problem(integrator, **kw)
+    sim = O.Simulation(prob, m0)
+    for _ in range(int(round(t_end / dt))):
+        sim.step(dt)
+    return sim.m
+
+
+@pytest.fixture(scope="module")
+def smooth_reference():
+    return _final_m(O.RK4, 1e-15, 4e-12)
+
+
+# measured rates: RK4 4.01, ABM3 2.89 (its Heun start-up steps still show at
+# this dt), Heun 2.00
+@pytest.mark.parametrize("integrator,order", [(O.RK4, 4), (O.ABM3, 3), (O.HEUN, 2)])
+def test_fixed_step_integrators_converge_at_their_order(integrator, order, smooth_reference):
+    e1 = np.abs(_final_m(integrator, 2e-14, 4e-12) - smooth_reference).max()
+    e2 = np.abs(_final_m(integrator, 1e-14, 4e-12) - smooth_reference).max()
+    rate = math.log2(e1 / e2)
+    assert order - 0.45 <= rate <= order + 0.45, (e1, e2, rate)
+
+
+def test_rk23_fixed_step_is_third_order(smooth_reference):
+    """max_error far above any error estimate makes every attempt accept, so
+    RK23 runs at the given dt (the clamps are set around it)."""
+    errs = []
+    for dt in (2e-14, 1e-14):
+        errs.append(np.abs(_final_m(O.RK23, dt, 4e-12, max_error=1e30, dt_min=1e-18, dt_max=1.0,
+                                    headroom=0.8) - smooth_reference).max())
+    rate = math.log2(errs[0] / errs[1])
+    assert 2.55 <= rate <= 3.45, (errs, rate)
+
+
+def test_abm3_startup_steps_are_heun_steps():
+    prob_h, m0 = _smooth_problem(O.HEUN)
+    prob_a, _ = _smooth_problem(O.ABM3)
+    h, a = O.Simulation(prob_h, m0), O.Simulation(prob_a, m0)
+    for _ in range(3):
+        rh, ra = h.step(1e-13), a.step(1e-13)
+        assert np.array_equal(h.m, a.m)
+        # energies are OpenMP reductions: summation order varies by a few ulp
+        assert abs(rh["e_total"] - ra["e_total"]) <= 1e-12 * abs(rh["e_total"])
+    h.step(1e-13)
+    a.step(1e-13)  # the first multistep step differs from Heun
+    assert not np.array_equal(h.m, a.m)
+
+
+def test_abm3_restarts_with_heun_when_dt_changes():
+    """More than 10 % change of dt: three Heun steps again, from the same state."""
+    prob_a, m0 = _smooth_problem(O.ABM3)
+    a = O.Simulation(prob_a, m0)
+    for _ in range(5):
+        a.step(1e-13)
+    prob_h, _ = _smooth_problem(O.HEUN)
+    h = O.Simulation(prob_h, a.m)  # (re-normalised on creation: last-bit changes only)
+    for _ in range(3):
+        a.step(1.5e-13)
+        h.step(1.5e-13)
+        assert np.abs(h.m - a.m).max() <= 1e-13
+    # a change of less than 10 % keeps the history
+    b = O.Simulation(prob_a, m0)
+    c = O.Simulation(prob_a, m0)
+    for _ in range(5):
+        b.step(1e-13)
+        c.step(1e-13)
+    b.step(1.05e-13)
+    h2 = O.Simulation(prob_h, c.m)
+    h2.step(1.05e-13)
+    assert np.abs(b.m - h2.m).max() > 1e-11
+
+
+def test_rk23_controller_rejects_and_suggests():
+    prob, m0 = _smooth_problem(O.RK23, max_error=1e-7, dt_min=1e-18, dt_max=1e-10, headroom=0.8)
+    sim = O.Simulation(prob, m0)
+    r = sim.step(5e-12)  # far too large for 1e-7: rejected at least once
+    assert r["rejected_attempts"] >= 1
+    assert r["dt_used"] < 5e-12
+    # the next suggestion follows headroom * dt * (max_error / err)^(1/3), clamped
+    assert 0.0 < r["suggested_next_dt"] <= 1e-10
+    dt = r["suggested_next_dt"]
+    r2 = sim.step(dt)
+    assert r2["dt_used"] == dt or r2["rejected_attempts"] > 0
