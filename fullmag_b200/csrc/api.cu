@@ -167,6 +167,64 @@ void projection_octant(Backend &b, std::vector<double> (&spec)[6]) {
             }
 }
 
+// Boundary tiers (fullmag_fdm.h:151-187; api.cpp:247-290, context.cu:629-730).
+// T0 uses the face links, T1 the intersection distances; both weight the demag
+// magnetisation by the volume fraction; the sparse demag correction needs a
+// tier.  Unlike the reference, which skips the tier silently when the volume
+// fraction is missing or has the wrong length, and reads out of bounds on bad
+// correction indices, these are errors here.
+static bool parse_boundary(Backend &b, const fullmag_fdm_plan_desc *plan) {
+    const int tier = (int)plan->boundary_correction;
+    if (tier == FULLMAG_FDM_BOUNDARY_NONE) return true;
+    if (tier != FULLMAG_FDM_BOUNDARY_VOLUME && tier != FULLMAG_FDM_BOUNDARY_FULL) {
+        b.last_error = "unknown boundary_correction " + std::to_string(tier);
+        return false;
+    }
+    if (!plan->volume_fraction) { b.last_error = "boundary_correction: volume_fraction is required"; return false; }
+    if (plan->volume_fraction_len != (uint64_t)b.n) {
+        b.last_error = "volume_fraction_len mismatch: expected " + std::to_string(b.n) + ", got " +
+                       std::to_string(plan->volume_fraction_len);
+        return false;
+    }
+    const size_t n = (size_t)b.n;
+    b.boundary_tier = tier;
+    b.phi_floor = plan->boundary_phi_floor > 0.0 ? plan->boundary_phi_floor : 0.05;
+    b.delta_min = plan->boundary_delta_min > 0.0 ? plan->boundary_delta_min : 0.1 * std::min({b.dx, b.dy, b.dz});
+    b.vf_host.assign(plan->volume_fraction, plan->volume_fraction + n);
+    const double *faces[6] = {plan->face_link_xp, plan->face_link_xm, plan->face_link_yp,
+                              plan->face_link_ym, plan->face_link_zp, plan->face_link_zm};
+    const double *deltas[6] = {plan->delta_xp, plan->delta_xm, plan->delta_yp,
+                               plan->delta_ym, plan->delta_zp, plan->delta_zm};
+    bool have_faces = true, have_deltas = true;
+    for (int q = 0; q < 6; ++q) {
+        have_faces = have_faces && faces[q];
+        have_deltas = have_deltas && deltas[q];
+    }
+    if (tier == FULLMAG_FDM_BOUNDARY_VOLUME && have_faces) {
+        b.ex_tier = 1;
+        b.face_host.resize(6 * n);
+        for (int q = 0; q < 6; ++q) std::copy(faces[q], faces[q] + n, b.face_host.begin() + q * n);
+    } else if (tier == FULLMAG_FDM_BOUNDARY_FULL && have_deltas) {
+        b.ex_tier = 2;
+        b.delta_host.resize(6 * n);
+        for (int q = 0; q < 6; ++q) std::copy(deltas[q], deltas[q] + n, b.delta_host.begin() + q * n);
+    }
+    if (plan->has_demag_boundary_corr && plan->demag_corr_target_idx && plan->demag_corr_source_idx &&
+        plan->demag_corr_tensor && plan->demag_corr_target_count > 0 && plan->demag_corr_stencil_size > 0) {
+        const size_t T = plan->demag_corr_target_count, S = plan->demag_corr_stencil_size;
+        b.corr_targets = (uint32_t)T;
+        b.corr_stencil = (uint32_t)S;
+        b.corr_tgt_host.assign(plan->demag_corr_target_idx, plan->demag_corr_target_idx + T);
+        b.corr_src_host.assign(plan->demag_corr_source_idx, plan->demag_corr_source_idx + T * S);
+        b.corr_ten_host.assign(plan->demag_corr_tensor, plan->demag_corr_tensor + T * S * 6);
+        for (int32_t v : b.corr_tgt_host)
+            if (v >= (int64_t)n) { b.last_error = "demag_corr_target_idx " + std::to_string(v) + " out of range"; return false; }
+        for (int32_t v : b.corr_src_host)
+            if (v >= (int64_t)n) { b.last_error = "demag_corr_source_idx " + std::to_string(v) + " out of range"; return false; }
+    }
+    return true;
+}
+
 bool create_impl(Backend &b, const fullmag_fdm_plan_desc *plan, const fullmag_fdm_plan_ext *ext) {
     // plan validation and host-side setup first: no CUDA call before the plan is accepted
     b.nx = (int)plan->grid.nx; b.ny = (int)plan->grid.ny; b.nz = (int)plan->grid.nz;
@@ -223,11 +281,7 @@ bool create_impl(Backend &b, const fullmag_fdm_plan_desc *plan, const fullmag_fd
                                std::to_string(i) + " exceeds the 256-entry exchange table";
                 return false;
             }
-    if (plan->boundary_correction != FULLMAG_FDM_BOUNDARY_NONE && plan->volume_fraction != nullptr &&
-        plan->volume_fraction_len == (uint64_t)b.n) {
-        b.last_error = "boundary correction tiers VOLUME/FULL are not implemented by this backend";
-        return false;
-    }
+    if (!parse_boundary(b, plan)) return false;
     fullmag_fdm_ext_demag_source demag_src = FULLMAG_FDM_EXT_DEMAG_FROM_PLAN;
     if (ext) {
         if (ext->struct_size < sizeof(fullmag_fdm_plan_ext)) { b.last_error = "fullmag_fdm_plan_ext.struct_size too small"; return false; }
@@ -241,6 +295,10 @@ bool create_impl(Backend &b, const fullmag_fdm_plan_desc *plan, const fullmag_fd
         demag_src = ext->demag_source;
     }
     if (!b.has_ms_map && !(b.ms > 0)) { b.last_error = "saturation_magnetisation must be positive"; return false; }
+    if (b.has_ms_map && b.boundary_tier) {
+        b.last_error = "a per-cell Ms map cannot be combined with boundary correction tiers";
+        return false;
+    }
     {
         // FULLMAG_FDM_FFT=stockham keeps the shared-memory Stockham FFT even for
         // power-of-two lengths (both FFT paths are covered by the parity tests)
@@ -320,6 +378,18 @@ bool create_impl(Backend &b, const fullmag_fdm_plan_desc *plan, const fullmag_fd
         if (!fm::cuda_ok(b, cudaMemcpy(b.d_lut, lut.data(), lut.size() * 8, cudaMemcpyHostToDevice), "upload lut")) return false;
     }
     if (b.has_ms_map && !fm::cuda_ok(b, cudaMemcpy(b.d_msmap, b.ms_map_host.data(), b.n * 8, cudaMemcpyHostToDevice), "upload ms_map")) return false;
+    if (b.boundary_tier) {
+        auto up = [&](void *dst, const void *src, size_t bytes, const char *what) {
+            return bytes == 0 || fm::cuda_ok(b, cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), what);
+        };
+        if (!up(b.d_vf, b.vf_host.data(), b.vf_host.size() * 8, "upload volume_fraction") ||
+            !up(b.d_face, b.face_host.data(), b.face_host.size() * 8, "upload face links") ||
+            !up(b.d_delta, b.delta_host.data(), b.delta_host.size() * 8, "upload deltas") ||
+            !up(b.d_corr_tgt, b.corr_tgt_host.data(), b.corr_tgt_host.size() * 4, "upload demag_corr_target_idx") ||
+            !up(b.d_corr_src, b.corr_src_host.data(), b.corr_src_host.size() * 4, "upload demag_corr_source_idx") ||
+            !up(b.d_corr_ten, b.corr_ten_host.data(), b.corr_ten_host.size() * 8, "upload demag_corr_tensor"))
+            return false;
+    }
     if (!fm::cuda_ok(b, cudaDeviceSynchronize(), "create sync")) return false;
     if (!fm::backend_upload_m_f64(b, plan->initial_magnetization_xyz, plan->initial_magnetization_len)) return false;
     if (!fm::backend_refresh(b)) return false;

@@ -154,6 +154,7 @@ struct Impl {
         a.mask = b.d_mask;
         a.ms_map = b.d_msmap;
         a.ms = b.ms;
+        a.vf = b.boundary_tier ? b.d_vf : nullptr;
         a.hd = (T *)hd;
         a.norm = 1.0 / ((double)b.Lx * (double)b.Ly * (double)b.Lz);
         a.lines_x = b.lines_x; a.lines_y = b.lines_y; a.kt_z = b.kt_z; a.kb_y = b.kb_y;
@@ -328,10 +329,23 @@ struct Impl {
         return ok;
     }
 
-    // H_d(m) into hd.
+    // H_d(m) into hd, then the sparse boundary correction when the plan has one.
     static bool demag(Backend &b, const void *m, void *hd) {
         if (!b.enable_demag) return true;
-        if (b.use_reg) return demag_reg(b, m, hd);
+        if (!(b.use_reg ? demag_reg(b, m, hd) : demag_stockham(b, m, hd))) return false;
+        if (b.corr_targets) {
+            {
+                ProfScope p(b, "demag_boundary_corr");
+                k_demag_corr<T><<<(b.corr_targets + 255) / 256, 256, 0, b.stream>>>(
+                    (const T *)m, (T *)hd, b.n, b.d_vf, b.d_corr_tgt, b.d_corr_src, b.d_corr_ten, b.ms,
+                    b.corr_targets, b.corr_stencil);
+            }
+            return check_launch(b, "demag boundary correction");
+        }
+        return true;
+    }
+
+    static bool demag_stockham(Backend &b, const void *m, void *hd) {
         DemagArgs<T> a = demag_args(b, m, hd);
         const int RB = 2 * b.lines_x;
         dim3 gx((b.ny + RB - 1) / RB, b.nz, 3);
@@ -342,9 +356,6 @@ struct Impl {
         if (b.thin) {
             ProfScope p(b, "demag_y_conv");
             k_y_conv<T><<<(b.nkx + b.kb_y - 1) / b.kb_y, 256, b.smem_yc, b.stream>>>(a);
-        } else if (b.use_yz) {
-            ProfScope p(b, "demag_yz");
-            if (!yz_launch(b, a)) return false;
         } else {
             const long long lines = 3LL * b.nz * b.nkx;
             const unsigned gy = (unsigned)((lines + b.lines_y - 1) / b.lines_y);
@@ -380,6 +391,13 @@ struct Impl {
         s.dinv[2] = 1.0 / (b.dz * b.dz);
         s.aex = b.aex; s.ms = b.ms; s.ms_map = b.d_msmap;
         s.ex_pref = 2.0 * b.aex / (kMu0 * b.ms);
+        s.ex_tier = b.ex_tier;
+        s.vf = b.d_vf;
+        s.face = b.d_face;
+        s.delta = b.d_delta;
+        s.phi_floor = b.phi_floor;
+        s.delta_min = b.delta_min;
+        s.cell[0] = b.dx; s.cell[1] = b.dy; s.cell[2] = b.dz;
         s.ex_pref_lut = 2.0 / (kMu0 * b.ms);
         s.mask = b.d_mask; s.region = b.d_region; s.lut = b.d_lut;
         s.enable_exchange = b.enable_exchange; s.enable_demag = b.enable_demag;
@@ -822,10 +840,21 @@ bool backend_alloc(Backend &b) {
         items.push_back({(void **)&b.d_lut, (size_t)256 * 256 * 8});
     }
     if (b.has_ms_map) items.push_back({(void **)&b.d_msmap, (size_t)b.n * 8});
+    if (b.boundary_tier) {
+        items.push_back({(void **)&b.d_vf, b.vf_host.size() * 8});
+        if (!b.face_host.empty()) items.push_back({(void **)&b.d_face, b.face_host.size() * 8});
+        if (!b.delta_host.empty()) items.push_back({(void **)&b.d_delta, b.delta_host.size() * 8});
+        if (b.corr_targets) {
+            items.push_back({(void **)&b.d_corr_tgt, b.corr_tgt_host.size() * 4});
+            items.push_back({(void **)&b.d_corr_src, b.corr_src_host.size() * 4});
+            items.push_back({(void **)&b.d_corr_ten, b.corr_ten_host.size() * 8});
+        }
+    }
     // stage kernels: the z-marching kernel serves a uniform material whose
     // 3 n fits 32-bit indices; its planes per thread (zb) are halved until the
     // grid has about 8 blocks per SM
-    b.stage_plain = !b.has_mask && !b.has_ms_map && !b.has_regions && 3ULL * (unsigned long long)b.n < (1ULL << 32);
+    b.stage_plain = !b.has_mask && !b.has_ms_map && !b.has_regions && !b.boundary_tier &&
+                    3ULL * (unsigned long long)b.n < (1ULL << 32);
     {
         auto blocks = [&](int zb) {
             return (long long)((b.nx + 31) / 32) * ((b.ny + kStagePlainBY - 1) / kStagePlainBY) * ((b.nz + zb - 1) / zb);

@@ -30,6 +30,17 @@ struct Backend {
     bool has_mask = false, has_regions = false, has_ms_map = false;
     std::vector<uint8_t> mask_host;
     std::vector<double> ms_map_host;
+    // boundary tiers (fullmag_fdm.h:151-187): tier as given; ex_tier the
+    // exchange actually used (1 needs the face links, 2 the distances, as the
+    // reference's launch conditions); phi-weighted demag whenever tier > 0
+    int boundary_tier = 0, ex_tier = 0;
+    double phi_floor = 0.05, delta_min = 0.0;
+    std::vector<double> vf_host, face_host, delta_host;  // [N], [6][N], [6][N] (xp, xm, yp, ym, zp, zm)
+    std::vector<int32_t> corr_tgt_host, corr_src_host;
+    std::vector<double> corr_ten_host;
+    uint32_t corr_targets = 0, corr_stencil = 0;
+    double *d_vf = nullptr, *d_face = nullptr, *d_delta = nullptr, *d_corr_ten = nullptr;
+    int32_t *d_corr_tgt = nullptr, *d_corr_src = nullptr;
     long long active_count = 0;
     double max_error = 1e-5, dt_min = 1e-18, dt_max = 1e-10, headroom = 0.8;
 

@@ -38,6 +38,7 @@ struct DemagArgs {
     const uint8_t *mask;    // may be null
     const double *ms_map;   // may be null (then ms)
     double ms;
+    const double *vf;       // boundary tiers: volume fraction (M = phi Ms m), else null
     T *hd;                  // SoA demag field out
     double norm;            // 1 / (Lx Ly Lz)
     int lines_x;            // complex lines (= 2 rows) per x-pass block
@@ -50,6 +51,15 @@ template <typename T>
 __device__ __forceinline__ bool cell_active(const DemagArgs<T> &a, long long i, double &ms_i) {
     ms_i = a.ms_map ? a.ms_map[i] : a.ms;
     return (!a.mask || a.mask[i] != 0) && (ms_i > 0.0);
+}
+
+// Magnetisation component fed to the FFT: (phi_i Ms) m_i over every cell when
+// a boundary tier weights it (demag_fp64.cu:79-85), else Ms_i m_i on active cells.
+template <typename T>
+__device__ __forceinline__ T demag_source(const DemagArgs<T> &a, long long i, T m) {
+    if (a.vf) return (T)((a.vf[i] * a.ms) * (double)m);
+    double msi;
+    return cell_active(a, i, msi) ? (T)((double)m * msi) : T(0);
 }
 
 // Apply H = -N(k) M(k) for one frequency (kx, ky, kz); M is overwritten by H.
@@ -97,8 +107,7 @@ __global__ void __launch_bounds__(256) k_x_fwd(DemagArgs<T> a) {
         T v = T(0);
         if (x < a.nx && y < a.ny) {
             const long long i = ((long long)z * a.ny + y) * a.nx + x;
-            double msi;
-            if (cell_active(a, i, msi)) v = (T)((double)mc[i] * msi);
+            v = demag_source(a, i, mc[i]);
         }
         T *line = reinterpret_cast<T *>(bufA + (r >> 1) * ld);
         line[2 * x + (r & 1)] = v;
@@ -310,6 +319,41 @@ __global__ void __launch_bounds__(256) k_x_inv(DemagArgs<T> a) {
         double msi;
         hc[i] = cell_active(a, i, msi) ? ((r & 1) ? v.y : v.x) * nrm : T(0);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Sparse demag boundary correction (demag_boundary_fp64.cu:20-76): for target
+// t, H(t) += -sum_s dN(t, s) M(s) with M(s) = (phi_s Ms) m_s and the tensor
+// components (xx, xy, xz, yy, yz, zz); negative indices are skipped.  One
+// thread per target, FP64 arithmetic, added to the field in its precision.
+// The targets are distinct cells (each is updated by one thread).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_demag_corr(const T *__restrict__ m, T *hd, long long n,
+                                                    const double *__restrict__ vf,
+                                                    const int32_t *__restrict__ tgt,
+                                                    const int32_t *__restrict__ src,
+                                                    const double *__restrict__ ten, double ms,
+                                                    unsigned targets, unsigned stencil) {
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= targets) return;
+    const int32_t ti = tgt[t];
+    if (ti < 0) return;
+    double cx_ = 0.0, cy_ = 0.0, cz_ = 0.0;
+    for (unsigned q = 0; q < stencil; ++q) {
+        const size_t pq = (size_t)t * stencil + q;
+        const int32_t si = src[pq];
+        if (si < 0) continue;
+        const double *N = ten + pq * 6;
+        const double w = vf[si] * ms;
+        const double Mx = w * (double)m[si], My = w * (double)m[n + si], Mz = w * (double)m[2 * n + si];
+        cx_ -= N[0] * Mx + N[1] * My + N[2] * Mz;
+        cy_ -= N[1] * Mx + N[3] * My + N[4] * Mz;
+        cz_ -= N[2] * Mx + N[4] * My + N[5] * Mz;
+    }
+    hd[ti] = (T)((double)hd[ti] + cx_);
+    hd[n + ti] = (T)((double)hd[n + ti] + cy_);
+    hd[2 * n + ti] = (T)((double)hd[2 * n + ti] + cz_);
 }
 
 }  // namespace fm

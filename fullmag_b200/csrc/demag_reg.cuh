@@ -43,13 +43,12 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
     const T msT = (T)a.ms;
     auto in = [&](int j) -> C {
         C v = mk<T>(0, 0);
-        if (!a.mask && !a.ms_map) {
+        if (!a.mask && !a.ms_map && !a.vf) {
             if (ya < ny) v.x = mc[rowa + j] * msT;
             if (yb < ny) v.y = mc[rowb + j] * msT;
         } else {
-            double msi;
-            if (ya < ny && cell_active(a, rowa + j, msi)) v.x = mc[rowa + j] * (T)msi;
-            if (yb < ny && cell_active(a, rowb + j, msi)) v.y = mc[rowb + j] * (T)msi;
+            if (ya < ny) v.x = demag_source(a, rowa + j, mc[rowa + j]);
+            if (yb < ny) v.y = demag_source(a, rowb + j, mc[rowb + j]);
         }
         return v;
     };

@@ -52,6 +52,12 @@ struct StageArgs {
     const uint8_t *mask;            // optional
     const uint32_t *region;         // optional
     const double *lut;              // 256 x 256, with region
+    int ex_tier;                    // boundary tiers: 0 standard, 1 T0 face links, 2 T1 ECB stencil
+    const double *vf;               // volume fraction [n] (tiers)
+    const double *face;             // [6][n] face link fractions xp, xm, yp, ym, zp, zm (T0)
+    const double *delta;            // [6][n] boundary distances, same order (T1)
+    double phi_floor, delta_min;
+    double cell[3];                 // dx, dy, dz
     int enable_exchange, enable_demag, has_ext;
     double hext[3], hac[3], ac_omega;
     double gamma_bar, alpha;
@@ -91,6 +97,71 @@ template <typename T>
 __device__ __forceinline__ bool st_active(const StageArgs<T> &a, long long i, double &ms_i) {
     ms_i = a.ms_map ? a.ms_map[i] : a.ms;
     return (!a.mask || a.mask[i] != 0) && (ms_i > 0.0);
+}
+
+// Exchange field of the boundary tiers at an active cell i = (x, y, z) with
+// m = c.  T0 (exchange_t0_fp64.cu:22-133): sum over the faces -x, +x, -y, +y,
+// -z, +z inside the grid of f (m_j - c) / d^2 with face link f > 0, times
+// 2A / (mu0 Ms) / max(phi, phi_floor).  T1 (exchange_t1_fp64.cu:28-175): per
+// neighbour with non-zero m, 2 (m_j - c) / (d (d + delta_opposite)), deltas
+// clamped below by delta_min, times 2A / (mu0 Ms).  The z faces are skipped for
+// nz = 1; cells with phi <= 0 or m = 0 get zero (the reference leaves them
+// unwritten).
+template <typename T>
+__device__ __forceinline__ void tier_exchange(const StageArgs<T> &a, long long i, int x, int y, int z,
+                                              const double (&c)[3], double (&h)[3]) {
+    h[0] = h[1] = h[2] = 0.0;
+    const double phi0 = a.vf[i];
+    if (phi0 <= 0.0 || (c[0] == 0.0 && c[1] == 0.0 && c[2] == 0.0)) return;
+    const long long n = a.n;
+    const int xyz[3] = {x, y, z}, ext[3] = {a.nx, a.ny, a.nz};
+    const long long str[3] = {1, a.nx, (long long)a.nx * a.ny};
+    double b[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        if (ax == 2 && a.nz <= 1) break;
+        const bool has_m = xyz[ax] > 0, has_p = xyz[ax] + 1 < ext[ax];
+        const double d = a.cell[ax];
+        if (a.ex_tier == 1) {
+            const double fm = a.face[(2 * ax + 1) * n + i], fp = a.face[2 * ax * n + i];
+            const double inv = a.dinv[ax];
+            if (fm > 0.0 && has_m) {
+                const long long j = i - str[ax];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) b[k] += fm * inv * ((double)a.m[k * n + j] - c[k]);
+            }
+            if (fp > 0.0 && has_p) {
+                const long long j = i + str[ax];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) b[k] += fp * inv * ((double)a.m[k * n + j] - c[k]);
+            }
+        } else {
+            const double dm = fmax(a.delta[(2 * ax + 1) * n + i], a.delta_min);
+            const double dp = fmax(a.delta[2 * ax * n + i], a.delta_min);
+            if (has_m && dm > 0.0) {
+                const long long j = i - str[ax];
+                const double mn[3] = {(double)a.m[j], (double)a.m[n + j], (double)a.m[2 * n + j]};
+                if (mn[0] != 0.0 || mn[1] != 0.0 || mn[2] != 0.0) {
+                    const double coeff = 2.0 / (d * (d + dp));
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) b[k] += coeff * (mn[k] - c[k]);
+                }
+            }
+            if (has_p && dp > 0.0) {
+                const long long j = i + str[ax];
+                const double mn[3] = {(double)a.m[j], (double)a.m[n + j], (double)a.m[2 * n + j]};
+                if (mn[0] != 0.0 || mn[1] != 0.0 || mn[2] != 0.0) {
+                    const double coeff = 2.0 / (d * (d + dm));
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) b[k] += coeff * (mn[k] - c[k]);
+                }
+            }
+        }
+    }
+    double sc = 2.0 * a.aex / (kMu0 * a.ms);
+    if (a.ex_tier == 1) sc = sc * (1.0 / (phi0 > a.phi_floor ? phi0 : a.phi_floor));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) h[k] = sc * b[k];
 }
 
 // Reduce acc[NQ] over the block and, in the last block to finish, over all
@@ -205,7 +276,9 @@ __global__ void __launch_bounds__(256, 3) k_stage(StageArgs<T> a) {
             R hxc[3] = {0.0, 0.0, 0.0};
             if (a.enable_exchange) {
                 const R ix2 = a.dinv[0], iy2 = a.dinv[1], iz2 = a.dinv[2];
-                if (!a.region) {
+                if (a.ex_tier) {
+                    tier_exchange(a, i, x, y, z, c3, hxc);
+                } else if (!a.region) {
                     const R pref = a.ms_map ? 2.0 * a.aex / (kMu0 * ms_i) : a.ex_pref;
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {

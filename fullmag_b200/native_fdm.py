@@ -27,6 +27,7 @@ MU0 = 4.0 * np.pi * 1e-7
 OK, ERR_INVALID, ERR_CUDA, ERR_INTERNAL = 0, -1, -2, -3
 PRECISION_SINGLE, PRECISION_DOUBLE = 1, 2
 HEUN, DP45, ABM3, RK4, RK23 = 1, 2, 3, 4, 5
+BOUNDARY_NONE, BOUNDARY_VOLUME, BOUNDARY_FULL = 0, 1, 2
 OBS_M, OBS_H_EX, OBS_H_DEMAG, OBS_H_EXT, OBS_H_EFF = 1, 2, 3, 4, 5
 SNAP_F32, SNAP_F64 = 1, 2
 DEMAG_FROM_PLAN, DEMAG_NEWELL = 0, 1
@@ -237,6 +238,16 @@ class FdmPlan:
     ac_field: Optional[Sequence[float]] = None
     ac_frequency_hz: float = 0.0
     demag_source: int = DEMAG_FROM_PLAN
+    # boundary tiers (fullmag_fdm.h:151-187): BOUNDARY_NONE / _VOLUME (T0) / _FULL (T1);
+    # per-cell arrays of N doubles, directions in the order xp, xm, yp, ym, zp, zm
+    boundary_correction: int = 0
+    boundary_phi_floor: float = 0.0
+    boundary_delta_min: float = 0.0
+    volume_fraction: Optional[np.ndarray] = None
+    face_links: Optional[Sequence[np.ndarray]] = None
+    deltas: Optional[Sequence[np.ndarray]] = None
+    # sparse demag correction: targets [T], sources [T, S], tensors [T, S, 6]
+    demag_corr: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -289,6 +300,35 @@ class FdmPlan:
         if self.adaptive is not None:
             (d.adaptive_max_error, d.adaptive_dt_min, d.adaptive_dt_max,
              d.adaptive_headroom) = (float(v) for v in self.adaptive)
+        d.boundary_correction = int(self.boundary_correction)
+        d.boundary_phi_floor = float(self.boundary_phi_floor)
+        d.boundary_delta_min = float(self.boundary_delta_min)
+
+        def dptr(arr):
+            a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+            keep.append(a)
+            return a.ctypes.data_as(_dp), a.size
+
+        if self.volume_fraction is not None:
+            d.volume_fraction, d.volume_fraction_len = dptr(self.volume_fraction)
+        dirs = ("xp", "xm", "yp", "ym", "zp", "zm")
+        if self.face_links is not None:
+            for nm, arr in zip(dirs, self.face_links):
+                setattr(d, f"face_link_{nm}", dptr(arr)[0])
+        if self.deltas is not None:
+            for nm, arr in zip(dirs, self.deltas):
+                setattr(d, f"delta_{nm}", dptr(arr)[0])
+        if self.demag_corr is not None:
+            tgt, src, ten = self.demag_corr
+            t = np.ascontiguousarray(tgt, dtype=np.int32).reshape(-1)
+            sr = np.ascontiguousarray(src, dtype=np.int32).reshape(-1)
+            keep.extend([t, sr])
+            d.has_demag_boundary_corr = 1
+            d.demag_corr_target_idx = t.ctypes.data_as(C.POINTER(C.c_int32))
+            d.demag_corr_source_idx = sr.ctypes.data_as(C.POINTER(C.c_int32))
+            d.demag_corr_tensor = dptr(ten)[0]
+            d.demag_corr_target_count = t.size
+            d.demag_corr_stencil_size = sr.size // max(t.size, 1)
         return d
 
     def to_ext(self) -> Optional[PlanExt]:

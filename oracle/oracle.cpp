@@ -401,6 +401,16 @@ struct Problem {
         return true;
     }
     double ms_at(size_t i) const { return msmap.empty() ? d.ms : msmap[i]; }
+
+    // Boundary tiers, with the reference's launch conditions
+    // (exchange_fp64.cu:159-198, demag_fp64.cu:299, 364): the T0 exchange needs
+    // the face links, the T1 exchange the distances; phi-weighted demag needs
+    // only the volume fraction; the sparse correction needs a tier.
+    std::vector<double> vf, face[6], delta[6];
+    std::vector<int32_t> ctgt, csrc;
+    std::vector<double> cten;
+    int ex_tier = 0;
+    double phi_floor = 0.05, delta_min = 0.0;
     size_t index(size_t x, size_t y, size_t z) const { return x + nx * (y + ny * z); }
 
     V3 hext_at(double time) const {
@@ -463,9 +473,68 @@ struct Problem {
     }
 
     // exchange_field_from_vectors (lib.rs:2247-2299) + region LUT (exchange_fp64.cu:80-114)
+    // T0, exchange_t0_fp64.cu:22-133: face-link-weighted differences over the
+    // faces in the order -x, +x, -y, +y, -z, +z, normalised by max(phi, floor).
+    // T1, exchange_t1_fp64.cu:28-175: the ECB stencil 2 / (d (d + delta_opposite))
+    // per interior neighbour with non-zero m, deltas clamped below by delta_min.
+    // Cells with phi <= 0 or m = 0 get H_ex = 0 (the reference leaves them unwritten).
+    void exchange_tier(const std::vector<V3> &mm, std::vector<V3> &out) const {
+        const double i2[3] = {1.0 / (d.dx * d.dx), 1.0 / (d.dy * d.dy), 1.0 / (d.dz * d.dz)};
+        const double dd[3] = {d.dx, d.dy, d.dz};
+        const double scale0 = 2.0 * d.aex / (MU0 * d.ms);
+#pragma omp parallel for
+        for (long fl = 0; fl < (long)n; ++fl) {
+            size_t f = (size_t)fl;
+            out[f] = {0, 0, 0};
+            if (!active(f)) continue;
+            const V3 c = mm[f];
+            const double phi0 = vf[f];
+            if (phi0 <= 0.0 || (c[0] == 0.0 && c[1] == 0.0 && c[2] == 0.0)) continue;
+            size_t xyz[3] = {f % nx, (f / nx) % ny, f / (nx * ny)};
+            const size_t ext[3] = {nx, ny, nz};
+            const size_t stride[3] = {1, nx, nx * ny};
+            V3 b = {0, 0, 0};
+            for (int ax = 0; ax < 3; ++ax) {
+                if (ax == 2 && nz <= 1) break;
+                const bool has_m = xyz[ax] > 0, has_p = xyz[ax] + 1 < ext[ax];
+                if (ex_tier == 1) {
+                    const double fm = face[2 * ax + 1][f], fp = face[2 * ax][f];
+                    if (fm > 0.0 && has_m) {
+                        const V3 &mn = mm[f - stride[ax]];
+                        for (int cc = 0; cc < 3; ++cc) b[cc] += fm * i2[ax] * (mn[cc] - c[cc]);
+                    }
+                    if (fp > 0.0 && has_p) {
+                        const V3 &mn = mm[f + stride[ax]];
+                        for (int cc = 0; cc < 3; ++cc) b[cc] += fp * i2[ax] * (mn[cc] - c[cc]);
+                    }
+                } else {
+                    const double dm = std::max(delta[2 * ax + 1][f], delta_min);
+                    const double dp = std::max(delta[2 * ax][f], delta_min);
+                    if (has_m && dm > 0.0) {
+                        const V3 &mn = mm[f - stride[ax]];
+                        if (mn[0] != 0.0 || mn[1] != 0.0 || mn[2] != 0.0) {
+                            const double coeff = 2.0 / (dd[ax] * (dd[ax] + dp));
+                            for (int cc = 0; cc < 3; ++cc) b[cc] += coeff * (mn[cc] - c[cc]);
+                        }
+                    }
+                    if (has_p && dp > 0.0) {
+                        const V3 &mn = mm[f + stride[ax]];
+                        if (mn[0] != 0.0 || mn[1] != 0.0 || mn[2] != 0.0) {
+                            const double coeff = 2.0 / (dd[ax] * (dd[ax] + dm));
+                            for (int cc = 0; cc < 3; ++cc) b[cc] += coeff * (mn[cc] - c[cc]);
+                        }
+                    }
+                }
+            }
+            const double sc = ex_tier == 1 ? scale0 * (1.0 / (phi0 > phi_floor ? phi0 : phi_floor)) : scale0;
+            out[f] = scale(b, sc);
+        }
+    }
+
     void exchange_field(const std::vector<V3> &mm, std::vector<V3> &out) const {
         out.assign(n, V3{0, 0, 0});
         if (!d.enable_exchange) return;
+        if (ex_tier) { exchange_tier(mm, out); return; }
         double dx2 = d.dx * d.dx, dy2 = d.dy * d.dy, dz2 = d.dz * d.dz;
 #pragma omp parallel for
         for (long fl = 0; fl < (long)n; ++fl) {
@@ -522,7 +591,10 @@ struct Problem {
                 for (size_t x = 0; x < nx; ++x) {
                     size_t s = index(x, y, z);
                     size_t dd = x + px * (y + py * z);
-                    V3 mo = active(s) ? scale(mm[s], ms_at(s)) : V3{0, 0, 0};
+                    // phi-weighted packing M = (phi Ms) m over every cell when a tier
+                    // is set (demag_fp64.cu:79-85), else the mask
+                    V3 mo = !vf.empty() ? scale(mm[s], vf[s] * ms_at(s))
+                            : active(s) ? scale(mm[s], ms_at(s)) : V3{0, 0, 0};
                     bmx[dd] = cplx(mo[0], 0.0);
                     bmy[dd] = cplx(mo[1], 0.0);
                     bmz[dd] = cplx(mo[2], 0.0);
@@ -551,6 +623,23 @@ struct Problem {
                                               bhz[s].real() * norm_}
                                          : V3{0, 0, 0};
                 }
+        // sparse boundary correction H(t) -= dN(t, s) M(s), demag_boundary_fp64.cu:20-76
+        const size_t S = d.corr_stencil;
+        for (size_t t = 0; t < ctgt.size(); ++t) {
+            const int32_t ti = ctgt[t];
+            if (ti < 0) continue;
+            V3 ch = {0, 0, 0};
+            for (size_t q = 0; q < S; ++q) {
+                const int32_t si = csrc[t * S + q];
+                if (si < 0) continue;
+                const double *N = &cten[(t * S + q) * 6];
+                const V3 M = scale(mm[(size_t)si], vf[(size_t)si] * ms_at((size_t)si));
+                ch[0] -= N[0] * M[0] + N[1] * M[1] + N[2] * M[2];
+                ch[1] -= N[1] * M[0] + N[3] * M[1] + N[4] * M[2];
+                ch[2] -= N[2] * M[0] + N[4] * M[1] + N[5] * M[2];
+            }
+            out[(size_t)ti] = add(out[(size_t)ti], ch);
+        }
     }
 
     void external_field(double time, std::vector<V3> &out) const {
@@ -990,6 +1079,27 @@ oracle_problem *oracle_create(const oracle_desc *desc, const double *m0) {
         p.lut.assign(256 * 256, 0.0);
         if (desc->exchange_lut) std::memcpy(p.lut.data(), desc->exchange_lut, 256 * 256 * sizeof(double));
         else for (size_t r = 0; r < 256; ++r) p.lut[r * 256 + r] = desc->aex;
+    }
+    if (desc->boundary_tier > 0 && desc->volume_fraction) {
+        p.vf.assign(desc->volume_fraction, desc->volume_fraction + p.n);
+        p.phi_floor = desc->phi_floor > 0.0 ? desc->phi_floor : 0.05;
+        p.delta_min = desc->delta_min > 0.0 ? desc->delta_min
+                                            : 0.1 * std::min(std::min(desc->dx, desc->dy), desc->dz);
+        bool faces = true, deltas = true;
+        for (int q = 0; q < 6; ++q) {
+            faces = faces && desc->face_link[q];
+            deltas = deltas && desc->delta[q];
+        }
+        if (faces) for (int q = 0; q < 6; ++q) p.face[q].assign(desc->face_link[q], desc->face_link[q] + p.n);
+        if (deltas) for (int q = 0; q < 6; ++q) p.delta[q].assign(desc->delta[q], desc->delta[q] + p.n);
+        p.ex_tier = (desc->boundary_tier == 1 && faces) ? 1 : (desc->boundary_tier >= 2 && deltas) ? 2 : 0;
+        if (desc->corr_target && desc->corr_source && desc->corr_tensor && desc->corr_targets > 0 &&
+            desc->corr_stencil > 0) {
+            const size_t T = desc->corr_targets, S = desc->corr_stencil;
+            p.ctgt.assign(desc->corr_target, desc->corr_target + T);
+            p.csrc.assign(desc->corr_source, desc->corr_source + T * S);
+            p.cten.assign(desc->corr_tensor, desc->corr_tensor + T * S * 6);
+        }
     }
     p.m.resize(p.n);
     for (size_t i = 0; i < p.n; ++i) {

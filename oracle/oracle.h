@@ -62,6 +62,20 @@ typedef struct {
      * octant mirrored with parity; the form the CUDA library stores) instead of
      * the reference's spectra, which carry rounding noise on the symmetry planes. */
     int symmetric_kernel;
+    /* Boundary tiers (native/include/fullmag_fdm.h:151-187): 0 none, 1 T0 (face-link
+     * exchange + phi-weighted demag), 2 T1 (ECB exchange + phi-weighted demag).
+     * Arrays are [N] doubles, directions in the order xp, xm, yp, ym, zp, zm. */
+    int boundary_tier;
+    double phi_floor, delta_min;   /* 0 -> 0.05 and 0.1 min(dx, dy, dz) */
+    const double *volume_fraction;
+    const double *face_link[6];
+    const double *delta[6];
+    /* sparse demag correction: targets [T], sources [T x S], tensors [T x S x 6]
+     * (xx, xy, xz, yy, yz, zz); negative indices are skipped */
+    const int32_t *corr_target;
+    const int32_t *corr_source;
+    const double *corr_tensor;
+    uint32_t corr_targets, corr_stencil;
 } oracle_desc;
 
 typedef struct {

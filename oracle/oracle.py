@@ -40,6 +40,12 @@ class OracleDesc(C.Structure):
         ("headroom", C.c_double),
         ("h_ac", C.c_double * 3), ("ac_freq", C.c_double),
         ("thin_film_2d", C.c_int), ("symmetric_kernel", C.c_int),
+        ("boundary_tier", C.c_int), ("phi_floor", C.c_double), ("delta_min", C.c_double),
+        ("volume_fraction", C.POINTER(C.c_double)),
+        ("face_link", C.POINTER(C.c_double) * 6), ("delta", C.POINTER(C.c_double) * 6),
+        ("corr_target", C.POINTER(C.c_int32)), ("corr_source", C.POINTER(C.c_int32)),
+        ("corr_tensor", C.POINTER(C.c_double)),
+        ("corr_targets", C.c_uint32), ("corr_stencil", C.c_uint32),
     ]
 
 
@@ -166,6 +172,16 @@ class Problem:
     ac_freq: float = 0.0
     thin_film_2d: bool = False
     symmetric_kernel: bool = False
+    # boundary tiers: 0 none, 1 T0, 2 T1; arrays [N], directions xp, xm, yp, ym, zp, zm
+    boundary_tier: int = 0
+    phi_floor: float = 0.0
+    delta_min: float = 0.0
+    volume_fraction: Optional[np.ndarray] = None
+    face_link: Optional[Sequence[np.ndarray]] = None
+    delta: Optional[Sequence[np.ndarray]] = None
+    corr_target: Optional[np.ndarray] = None
+    corr_source: Optional[np.ndarray] = None   # [T, S]
+    corr_tensor: Optional[np.ndarray] = None   # [T, S, 6] xx, xy, xz, yy, yz, zz
     _keep: list = field(default_factory=list, repr=False)
 
     def desc(self) -> OracleDesc:
@@ -204,6 +220,34 @@ class Problem:
             self.max_error, self.dt_min, self.dt_max, self.headroom)
         d.thin_film_2d = int(self.thin_film_2d)
         d.symmetric_kernel = int(self.symmetric_kernel)
+        d.boundary_tier = int(self.boundary_tier)
+        d.phi_floor, d.delta_min = self.phi_floor, self.delta_min
+
+        def keep_d(a):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            self._keep.append(a)
+            return _dptr(a)
+
+        def keep_i(a):
+            a = np.ascontiguousarray(a, dtype=np.int32)
+            self._keep.append(a)
+            return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+        if self.volume_fraction is not None:
+            d.volume_fraction = keep_d(self.volume_fraction)
+        for q in range(6):
+            if self.face_link is not None:
+                d.face_link[q] = keep_d(self.face_link[q])
+            if self.delta is not None:
+                d.delta[q] = keep_d(self.delta[q])
+        if self.corr_target is not None:
+            t = np.asarray(self.corr_target)
+            src = np.asarray(self.corr_source)
+            d.corr_target = keep_i(t)
+            d.corr_source = keep_i(src.reshape(-1))
+            d.corr_tensor = keep_d(np.asarray(self.corr_tensor).reshape(-1))
+            d.corr_targets = t.size
+            d.corr_stencil = src.size // max(t.size, 1)
         return d
 
 

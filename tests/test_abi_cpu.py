@@ -82,9 +82,11 @@ def _bad_plan_error(**kw):
     plan = nf.FdmPlan(**base)
     lib = nf.load_library()
     desc = plan.to_desc()
-    if "tamper" in kw:
-        pass
-    h = lib.fullmag_fdm_backend_create(C.byref(desc))
+    ext = plan.to_ext()
+    if ext is None:
+        h = lib.fullmag_fdm_backend_create(C.byref(desc))
+    else:
+        h = lib.fullmag_fdm_backend_create_ext(C.byref(desc), C.byref(ext))
     assert h is not None
     err = lib.fullmag_fdm_backend_last_error(h)
     lib.fullmag_fdm_backend_destroy(h)
@@ -101,6 +103,22 @@ def test_validation_errors_without_device():
     assert "spectrum_len mismatch" in _bad_plan_error(enable_demag=True, demag_spectra=[np.zeros(10)] * 6)
     assert "prime factor" in _bad_plan_error(cells=(11, 3, 2), initial_magnetization=np.zeros(3 * 66),
                                              enable_demag=True)
+
+
+def test_boundary_tier_validation_without_device():
+    """Boundary tiers: the reference skips a tier silently when the volume
+    fraction is missing or has the wrong length, and reads out of bounds on
+    bad correction indices; here these are create errors."""
+    ones = np.ones(24)
+    assert "unknown boundary_correction" in _bad_plan_error(boundary_correction=7, volume_fraction=ones)
+    assert "volume_fraction is required" in _bad_plan_error(boundary_correction=nf.BOUNDARY_VOLUME)
+    assert "volume_fraction_len mismatch" in _bad_plan_error(boundary_correction=nf.BOUNDARY_FULL,
+                                                             volume_fraction=np.ones(5))
+    corr = (np.array([3], np.int32), np.array([[2, 99]], np.int32), np.zeros((1, 2, 6)))
+    assert "demag_corr_source_idx 99 out of range" in _bad_plan_error(
+        boundary_correction=nf.BOUNDARY_VOLUME, volume_fraction=ones, demag_corr=corr)
+    assert "per-cell Ms map" in _bad_plan_error(boundary_correction=nf.BOUNDARY_VOLUME, volume_fraction=ones,
+                                                ms_map=np.full(24, 8e5))
 
 
 @pytest.mark.parametrize("dims", [(5, 4, 3), (8, 6, 1), (16, 8, 2), (45, 3, 1)])

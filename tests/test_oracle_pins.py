@@ -362,3 +362,57 @@ def test_rk23_controller_rejects_and_suggests():
     dt = r["suggested_next_dt"]
     r2 = sim.step(dt)
     assert r2["dt_used"] == dt or r2["rejected_attempts"] > 0
+
+
+# ---------------------------------------------------------------- boundary tiers
+# exchange_t0_fp64.cu, exchange_t1_fp64.cu, demag_fp64.cu:79-85,
+# demag_boundary_fp64.cu.  The reference has no tests for the tiers; the
+# restatement is pinned by the interior limit (phi = 1, full faces, distances =
+# cell size: the tiers must reproduce the standard fields) and by the sparse
+# correction adding exactly -dN M at its targets.
+def _tier_problem(tier, nx=12, ny=10, nz=3, **kw):
+    n = nx * ny * nz
+    d = (2e-9, 2.5e-9, 3e-9)
+    vf = np.ones(n)
+    faces = [np.ones(n) for _ in range(6)]
+    deltas = [np.full(n, d[q // 2]) for q in range(6)]
+    prob = O.Problem(nx, ny, nz, *d, alpha=0.1, h_ext=(1e4, -2e4, 5e3), boundary_tier=tier,
+                     volume_fraction=vf, face_link=faces, delta=deltas, **kw)
+    return prob, O.random_unit_vectors(9, n)
+
+
+@pytest.mark.parametrize("tier", [1, 2])
+def test_tier_interior_limit_equals_standard_fields(tier):
+    prob, m0 = _tier_problem(tier)
+    base, _ = _tier_problem(0)
+    a = O.Simulation(prob, m0).observe()
+    b = O.Simulation(base, m0).observe()
+    for key in ("h_ex", "h_demag", "h_eff"):
+        scale = np.abs(b[key]).max()
+        assert np.abs(a[key] - b[key]).max() <= 1e-12 * scale, key
+
+
+def test_tier_demag_correction_adds_minus_dn_m():
+    rng = np.random.default_rng(3)
+    prob, m0 = _tier_problem(1)
+    n = prob.nx * prob.ny * prob.nz
+    targets = np.array([5, 17, 40, 77], np.int32)
+    sources = rng.integers(-1, n, size=(4, 5)).astype(np.int32)
+    tensors = rng.uniform(-1e-3, 1e-3, size=(4, 5, 6))
+    plain = O.Simulation(prob, m0)
+    prob.corr_target, prob.corr_source, prob.corr_tensor = targets, sources, tensors
+    corr = O.Simulation(prob, m0)
+    h0 = plain.observe()["h_demag"].reshape(-1, 3)
+    h1 = corr.observe()["h_demag"].reshape(-1, 3)
+    m = plain.m.reshape(-1, 3)
+    want = np.zeros_like(h0)
+    for t, ti in enumerate(targets):
+        for q, si in enumerate(sources[t]):
+            if si < 0:
+                continue
+            xx, xy, xz, yy, yz, zz = tensors[t, q]
+            N = np.array([[xx, xy, xz], [xy, yy, yz], [xz, yz, zz]])
+            want[ti] -= N @ (prob.ms * 1.0 * m[si])
+    assert np.abs((h1 - h0) - want).max() <= 1e-12 * np.abs(h0).max()
+    untouched = np.setdiff1d(np.arange(n), targets)
+    assert np.array_equal(h1[untouched], h0[untouched])
