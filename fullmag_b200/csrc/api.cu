@@ -476,6 +476,58 @@ int fullmag_fdm_backend_step_n(fullmag_fdm_backend *h, double dt, uint32_t n_ste
     return FULLMAG_FDM_OK;
 }
 
+int fullmag_fdm_adjoint_forward(fullmag_fdm_backend *h, double dt, uint32_t n_steps,
+                                uint32_t checkpoint_every, fullmag_fdm_step_stats *out) {
+    if (!h || !out || n_steps == 0) return FULLMAG_FDM_ERR_INVALID;
+    Backend &b = h->b;
+    if (!(dt > 0.0) || !std::isfinite(dt)) { b.last_error = "dt must be positive and finite"; return FULLMAG_FDM_ERR_INVALID; }
+    if (!ready(b)) return FULLMAG_FDM_ERR_INVALID;
+    if (b.integrator != FULLMAG_FDM_INTEGRATOR_HEUN) {
+        b.last_error = "the adjoint is implemented for the Heun integrator";
+        return FULLMAG_FDM_ERR_INVALID;
+    }
+    if (b.has_regions || b.boundary_tier) {
+        b.last_error = "the adjoint does not support region exchange tables or boundary tiers";
+        return FULLMAG_FDM_ERR_INVALID;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    fullmag_fdm_step_stats st{};
+    if (!fm::backend_adjoint_forward(b, dt, n_steps, checkpoint_every, &st)) return FULLMAG_FDM_ERR_CUDA;
+    st.wall_time_ns = (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                          std::chrono::steady_clock::now() - t0).count();
+    *out = st;
+    return FULLMAG_FDM_OK;
+}
+
+int fullmag_fdm_adjoint_backward(fullmag_fdm_backend *h, const double *dl_dm, uint64_t len, double *dl_dms,
+                                 double *dl_dh_ext, double *dl_dh_ac, double *dl_dm0) {
+    if (!h || !dl_dm) return FULLMAG_FDM_ERR_INVALID;
+    Backend &b = h->b;
+    if (len != (uint64_t)b.n * 3) { b.last_error = "out_len mismatch"; return FULLMAG_FDM_ERR_INVALID; }
+    if (!ready(b)) return FULLMAG_FDM_ERR_INVALID;
+    if (!b.adj_ready || b.step_count != b.adj_step_final || b.time != b.adj_t_final) {
+        b.last_error = "no recorded trajectory ends at the current state (call fullmag_fdm_adjoint_forward first)";
+        return FULLMAG_FDM_ERR_INVALID;
+    }
+    const size_t n = (size_t)b.n;
+    std::vector<double> lam(3 * n), gms(n), ghext(3 * n), ghac(3 * n), lam0(3 * n);
+    for (size_t i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) lam[c * n + i] = dl_dm[3 * i + c];
+    if (!fm::backend_adjoint_backward(b, lam.data(), gms.data(), ghext.data(), ghac.data(), lam0.data()))
+        return FULLMAG_FDM_ERR_CUDA;
+    if (dl_dms) std::copy(gms.begin(), gms.end(), dl_dms);
+    for (int c = 0; c < 3; ++c) {
+        double se = 0.0, sa = 0.0;  // fixed order: deterministic
+        for (size_t i = 0; i < n; ++i) { se += ghext[c * n + i]; sa += ghac[c * n + i]; }
+        if (dl_dh_ext) dl_dh_ext[c] = se;
+        if (dl_dh_ac) dl_dh_ac[c] = sa;
+    }
+    if (dl_dm0)
+        for (size_t i = 0; i < n; ++i)
+            for (int c = 0; c < 3; ++c) dl_dm0[3 * i + c] = lam0[c * n + i];
+    return FULLMAG_FDM_OK;
+}
+
 int fullmag_fdm_backend_copy_field_f64(fullmag_fdm_backend *h, fullmag_fdm_observable obs,
                                        double *out, uint64_t len) {
     if (!h || !out) return FULLMAG_FDM_ERR_INVALID;

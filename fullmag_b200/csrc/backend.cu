@@ -25,6 +25,7 @@
 #include "demag_yz.hpp"
 #include "newell_host.hpp"
 #include "stages.cuh"
+#include "adjoint.cuh"
 
 namespace fm {
 
@@ -141,7 +142,7 @@ template <typename T>
 struct Impl {
     using C = cx<T>;
 
-    static DemagArgs<T> demag_args(Backend &b, const void *m, void *hd) {
+    static DemagArgs<T> demag_args(Backend &b, const void *m, void *hd, bool unit = false) {
         DemagArgs<T> a{};
         a.nx = b.nx; a.ny = b.ny; a.nz = b.nz; a.n = b.n;
         a.Lx = b.Lx; a.Ly = b.Ly; a.Lz = b.Lz; a.nkx = b.nkx;
@@ -155,6 +156,7 @@ struct Impl {
         a.ms_map = b.d_msmap;
         a.ms = b.ms;
         a.vf = b.boundary_tier ? b.d_vf : nullptr;
+        a.unit_source = unit ? 1 : 0;
         a.hd = (T *)hd;
         a.norm = 1.0 / ((double)b.Lx * (double)b.Ly * (double)b.Lz);
         a.lines_x = b.lines_x; a.lines_y = b.lines_y; a.kt_z = b.kt_z; a.kb_y = b.kb_y;
@@ -217,8 +219,8 @@ struct Impl {
         return ok;
     }
 
-    static bool demag_reg(Backend &b, const void *m, void *hd) {
-        DemagArgs<T> a = demag_args(b, m, hd);
+    static bool demag_reg(Backend &b, const void *m, void *hd, bool unit = false) {
+        DemagArgs<T> a = demag_args(b, m, hd, unit);
         const int RB = 2 * b.lines_x;
         dim3 gx((b.ny + RB - 1) / RB, b.nz, 3);
         with_split(b.Lx, [&](auto l1, auto l2) {
@@ -330,9 +332,10 @@ struct Impl {
     }
 
     // H_d(m) into hd, then the sparse boundary correction when the plan has one.
-    static bool demag(Backend &b, const void *m, void *hd) {
+    // unit: the source is m itself on active cells (no Ms), for the adjoint.
+    static bool demag(Backend &b, const void *m, void *hd, bool unit = false) {
         if (!b.enable_demag) return true;
-        if (!(b.use_reg ? demag_reg(b, m, hd) : demag_stockham(b, m, hd))) return false;
+        if (!(b.use_reg ? demag_reg(b, m, hd, unit) : demag_stockham(b, m, hd, unit))) return false;
         if (b.corr_targets) {
             {
                 ProfScope p(b, "demag_boundary_corr");
@@ -345,8 +348,8 @@ struct Impl {
         return true;
     }
 
-    static bool demag_stockham(Backend &b, const void *m, void *hd) {
-        DemagArgs<T> a = demag_args(b, m, hd);
+    static bool demag_stockham(Backend &b, const void *m, void *hd, bool unit) {
+        DemagArgs<T> a = demag_args(b, m, hd, unit);
         const int RB = 2 * b.lines_x;
         dim3 gx((b.ny + RB - 1) / RB, b.nz, 3);
         {
@@ -449,6 +452,22 @@ struct Impl {
             launch_stage<MODE_EVAL>(b, s);
         }
         return check_launch(b, "stage_eval");
+    }
+
+    // k = RHS(m, t) with H_ex and H_eff written to the given buffers (adjoint).
+    static bool eval_fields(Backend &b, const void *m, double t, void *kout, void *hex, void *heff) {
+        StageArgs<T> s = stage_args(b, m, t);
+        s.kout = (T *)kout;
+        s.hex_out = (T *)hex;
+        s.heff_out = (T *)heff;
+        s.partials = nullptr;
+        s.counter = b.counter;
+        s.out = b.d_out;
+        {
+            ProfScope p(b, "stage_eval");
+            launch_stage<MODE_EVAL>(b, s);
+        }
+        return check_launch(b, "stage_eval (adjoint)");
     }
 
     static bool combine(Backend &b, int form, const void *m0, std::initializer_list<void *> ks,
@@ -720,6 +739,161 @@ struct Impl {
         return finish_step(b, dt, st, readback);
     }
 
+    // ------------------------------------------------------------------
+    // Adjoint of a Heun trajectory (adjoint.cuh).  Device layout of adj_mem:
+    // nck checkpoints and K segment states (3N T each), then the T work
+    // buffers k1, k2, m_p, H1, hex1, H2, hex2, lambda_H, hadj, final (3N each), then
+    // the FP64 buffers lambda, acc, gk, lloc, part, g_hext, g_hac (3N each) and
+    // g_ms (N).
+    // ------------------------------------------------------------------
+    struct AdjPtrs {
+        T *ck, *seg, *k1, *k2, *mp, *H1, *hex1, *H2, *hex2, *lh, *hadj, *fin;
+        double *lam, *acc, *gk, *lloc, *part, *ghext, *ghac, *gms;
+    };
+
+    static size_t adj_need(const Backend &b, uint32_t nck, uint32_t K) {
+        const size_t v = (size_t)3 * b.n;
+        return (size_t)(nck + K + 10) * v * sizeof(T) + (7 * v + (size_t)b.n) * sizeof(double) + 1024;
+    }
+
+    static AdjPtrs adj_ptrs(Backend &b) {
+        const size_t v = (size_t)3 * b.n;
+        AdjPtrs p{};
+        T *t = (T *)b.adj_mem;
+        p.ck = t; t += (size_t)b.adj_nck * v;
+        p.seg = t; t += (size_t)b.adj_K * v;
+        T **tb[10] = {&p.k1, &p.k2, &p.mp, &p.H1, &p.hex1, &p.H2, &p.hex2, &p.lh, &p.hadj, &p.fin};
+        for (T **q : tb) { *q = t; t += v; }
+        uintptr_t al = ((uintptr_t)t + 255) & ~(uintptr_t)255;
+        double *d = (double *)al;
+        double **db[7] = {&p.lam, &p.acc, &p.gk, &p.lloc, &p.part, &p.ghext, &p.ghac};
+        for (double **q : db) { *q = d; d += v; }
+        p.gms = d;
+        return p;
+    }
+
+    static AdjArgs adj_args(const Backend &b, double dt) {
+        AdjArgs a{};
+        a.n = b.n; a.nx = b.nx; a.ny = b.ny; a.nz = b.nz;
+        a.dinv[0] = 1.0 / (b.dx * b.dx); a.dinv[1] = 1.0 / (b.dy * b.dy); a.dinv[2] = 1.0 / (b.dz * b.dz);
+        a.aex = b.enable_exchange ? b.aex : 0.0;
+        a.ms = b.ms;
+        a.gamma_bar = b.gamma / (1.0 + b.alpha * b.alpha);
+        a.alpha = b.alpha;
+        a.pr = b.precession ? 1.0 : 0.0;
+        a.ms_map = b.d_msmap;
+        a.mask = b.d_mask;
+        a.dt = dt;
+        return a;
+    }
+
+    // Run n Heun steps from the current state, keeping every K-th state.
+    static bool adjoint_forward(Backend &b, double dt, uint32_t n, uint32_t K, fullmag_fdm_step_stats *st) {
+        if (K == 0) K = (uint32_t)std::ceil(std::sqrt((double)n));
+        K = std::max<uint32_t>(1, std::min(K, n));
+        const uint32_t nck = (n + K - 1) / K;
+        const size_t need = adj_need(b, nck, K);
+        if (need > b.adj_bytes) {
+            if (b.adj_mem) cudaFree(b.adj_mem);
+            b.adj_mem = nullptr;
+            b.adj_bytes = 0;
+            if (!cuda_ok(b, cudaMalloc(&b.adj_mem, need), "cudaMalloc(adjoint)")) return false;
+            b.adj_bytes = need;
+        }
+        b.adj_n = n; b.adj_K = K; b.adj_nck = nck; b.adj_dt = dt;
+        b.adj_ck_time.assign(nck, 0.0);
+        b.adj_ck_step.assign(nck, 0);
+        b.adj_ready = false;
+        AdjPtrs p = adj_ptrs(b);
+        const size_t vb = (size_t)3 * b.n * sizeof(T);
+        for (uint32_t s = 0; s < n; ++s) {
+            if (s % K == 0) {
+                const uint32_t c = s / K;
+                if (!cuda_ok(b, cudaMemcpyAsync(p.ck + (size_t)c * 3 * b.n, b.m, vb, cudaMemcpyDeviceToDevice, b.stream), "checkpoint"))
+                    return false;
+                b.adj_ck_time[c] = b.time;
+                b.adj_ck_step[c] = b.step_count;
+            }
+            if (!heun(b, dt, st, s + 1 == n)) return false;
+        }
+        b.adj_t_final = b.time;
+        b.adj_step_final = b.step_count;
+        b.adj_ready = true;
+        return true;
+    }
+
+    // One step's pull-back from lam (cotangent of m_{n+1}) to lam (of m_n).
+    static bool adjoint_step(Backend &b, AdjPtrs &p, const T *mn, double tn, double dt) {
+        const AdjArgs a = adj_args(b, dt);
+        const unsigned g = grid_cells(b);
+        const double omega = 2.0 * kPi * b.ac_freq;
+        // forward quantities of the step
+        if (!demag(b, mn, b.hd) || !eval_fields(b, mn, tn, p.k1, p.hex1, p.H1)) return false;
+        if (!combine(b, 0, mn, {(void *)p.k1}, {dt}, dt, p.mp)) return false;
+        const double t2 = tn + dt;
+        if (!demag(b, p.mp, b.hd) || !eval_fields(b, p.mp, t2, p.k2, p.hex2, p.H2)) return false;
+        // corrector normalisation, then stage 2 (at m_p, t + dt)
+        k_adj_start<T><<<g, 256, 0, b.stream>>>(a, mn, p.k1, p.k2, p.lam, p.acc, p.gk);
+        k_adj_vjp<T><<<g, 256, 0, b.stream>>>(a, p.mp, p.H2, p.gk, p.lh, p.lloc);
+        if (!demag(b, p.lh, p.hadj, true)) return false;
+        k_adj_apply<T><<<g, 256, 0, b.stream>>>(a, p.mp, p.lh, p.hadj, p.hex2, p.lloc, p.part, p.gms,
+                                                p.ghext, p.ghac, omega != 0.0 ? std::sin(t2 * omega) : 0.0);
+        // predictor normalisation, then stage 1 (at m_n, t)
+        k_adj_pred<T><<<g, 256, 0, b.stream>>>(a, mn, p.k1, p.part, p.acc, p.gk);
+        k_adj_vjp<T><<<g, 256, 0, b.stream>>>(a, mn, p.H1, p.gk, p.lh, p.lloc);
+        if (!demag(b, p.lh, p.hadj, true)) return false;
+        k_adj_apply<T><<<g, 256, 0, b.stream>>>(a, mn, p.lh, p.hadj, p.hex1, p.lloc, p.part, p.gms,
+                                                p.ghext, p.ghac, omega != 0.0 ? std::sin(tn * omega) : 0.0);
+        k_adj_finish<<<g, 256, 0, b.stream>>>(3LL * b.n, p.acc, p.part, p.lam);
+        return check_launch(b, "adjoint step");
+    }
+
+    // Pull dL/dm(final) back through the recorded trajectory.  The seed and the
+    // outputs are host FP64 buffers: lam (SoA 3N), dL/dMs per cell (N), the
+    // per-cell dL/dH_ext and dL/dH_ac (SoA 3N, summed by the caller), dL/dm0 (SoA 3N).
+    static bool adjoint_backward(Backend &b, const double *lam_soa_host, double *gms_host,
+                                 double *ghext_host, double *ghac_host, double *lam0_host) {
+        AdjPtrs p = adj_ptrs(b);
+        const size_t v = (size_t)3 * b.n;
+        const size_t vb = v * sizeof(T);
+        if (!cuda_ok(b, cudaMemcpyAsync(p.lam, lam_soa_host, v * 8, cudaMemcpyHostToDevice, b.stream), "adjoint seed") ||
+            !cuda_ok(b, cudaMemsetAsync(p.ghext, 0, v * 8, b.stream), "adjoint zero") ||
+            !cuda_ok(b, cudaMemsetAsync(p.ghac, 0, v * 8, b.stream), "adjoint zero") ||
+            !cuda_ok(b, cudaMemsetAsync(p.gms, 0, (size_t)b.n * 8, b.stream), "adjoint zero"))
+            return false;
+        // the final state is kept aside while the segments are replayed
+        bool ok = cuda_ok(b, cudaMemcpyAsync(p.fin, b.m, vb, cudaMemcpyDeviceToDevice, b.stream), "save final");
+        std::vector<double> seg_time(b.adj_K);
+        fullmag_fdm_step_stats st{};
+        for (int c = (int)b.adj_nck - 1; ok && c >= 0; --c) {
+            const uint32_t s0 = (uint32_t)c * b.adj_K;
+            const uint32_t len = std::min(b.adj_K, b.adj_n - s0);
+            ok = cuda_ok(b, cudaMemcpyAsync(b.m, p.ck + (size_t)c * v, vb, cudaMemcpyDeviceToDevice, b.stream), "restore checkpoint");
+            b.time = b.adj_ck_time[c];
+            b.step_count = b.adj_ck_step[c];
+            b.k1_valid = false;
+            for (uint32_t j = 0; ok && j < len; ++j) {
+                ok = cuda_ok(b, cudaMemcpyAsync(p.seg + (size_t)j * v, b.m, vb, cudaMemcpyDeviceToDevice, b.stream), "segment");
+                seg_time[j] = b.time;
+                if (ok && j + 1 < len) ok = heun(b, b.adj_dt, &st, false);
+            }
+            for (int j = (int)len - 1; ok && j >= 0; --j)
+                ok = adjoint_step(b, p, p.seg + (size_t)j * v, seg_time[j], b.adj_dt);
+        }
+        // restore the final state
+        if (ok) ok = cuda_ok(b, cudaMemcpyAsync(b.m, p.fin, vb, cudaMemcpyDeviceToDevice, b.stream), "restore final");
+        b.time = b.adj_t_final;
+        b.step_count = b.adj_step_final;
+        b.k1_valid = false;
+        b.obs_valid = false;
+        if (!ok) return false;
+        if (gms_host && !cuda_ok(b, cudaMemcpyAsync(gms_host, p.gms, (size_t)b.n * 8, cudaMemcpyDeviceToHost, b.stream), "dL/dMs")) return false;
+        if (ghext_host && !cuda_ok(b, cudaMemcpyAsync(ghext_host, p.ghext, v * 8, cudaMemcpyDeviceToHost, b.stream), "dL/dH_ext")) return false;
+        if (ghac_host && !cuda_ok(b, cudaMemcpyAsync(ghac_host, p.ghac, v * 8, cudaMemcpyDeviceToHost, b.stream), "dL/dH_ac")) return false;
+        if (lam0_host && !cuda_ok(b, cudaMemcpyAsync(lam0_host, p.lam, v * 8, cudaMemcpyDeviceToHost, b.stream), "dL/dm0")) return false;
+        return cuda_ok(b, cudaStreamSynchronize(b.stream), "adjoint sync");
+    }
+
     static bool refresh(Backend &b) {
         if (!demag(b, b.m, b.hd)) return false;
         if (!eval(b, b.m, b.time, b.k[0], false, true)) return false;
@@ -969,6 +1143,22 @@ bool backend_step_n(Backend &b, double dt, uint32_t nsteps, fullmag_fdm_step_sta
     return ok;
 }
 
+bool backend_adjoint_forward(Backend &b, double dt, uint32_t n, uint32_t K, fullmag_fdm_step_stats *st) {
+    const bool ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::adjoint_forward(b, dt, n, K, st)
+                                                                : Impl<float>::adjoint_forward(b, dt, n, K, st);
+    if (b.profiling) prof_collect(b);
+    return ok;
+}
+
+bool backend_adjoint_backward(Backend &b, const double *lam_soa, double *gms, double *ghext, double *ghac,
+                              double *lam0_soa) {
+    const bool ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE
+                        ? Impl<double>::adjoint_backward(b, lam_soa, gms, ghext, ghac, lam0_soa)
+                        : Impl<float>::adjoint_backward(b, lam_soa, gms, ghext, ghac, lam0_soa);
+    if (b.profiling) prof_collect(b);
+    return ok;
+}
+
 // Field pointer for an observable (after making H_ex / H_eff current).
 static const void *observable_ptr(Backend &b, fullmag_fdm_observable obs, bool &ok) {
     ok = true;
@@ -1138,6 +1328,8 @@ void backend_free(Backend &b) {
     b.prof_pending.clear();
     if (b.arena) cudaFree(b.arena);
     b.arena = nullptr;
+    if (b.adj_mem) cudaFree(b.adj_mem);
+    b.adj_mem = nullptr;
     if (b.h_out) cudaFreeHost(b.h_out);
     b.h_out = nullptr;
     if (b.stream) cudaStreamDestroy(b.stream);

@@ -58,6 +58,16 @@ struct Backend {
     size_t scalar = 8;        // bytes per state scalar
     void *m = nullptr, *mstage = nullptr, *hd = nullptr;
     void *k[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    // adjoint of a Heun trajectory (fullmag_fdm_adjoint_forward / _backward)
+    void *adj_mem = nullptr;      // one device block: checkpoints, segment, work buffers
+    size_t adj_bytes = 0;
+    uint32_t adj_n = 0, adj_K = 0, adj_nck = 0;
+    double adj_dt = 0.0;
+    std::vector<double> adj_ck_time;   // b.time at each checkpoint
+    std::vector<uint64_t> adj_ck_step; // step_count at each checkpoint
+    double adj_t_final = 0.0;
+    uint64_t adj_step_final = 0;
+    bool adj_ready = false;
     int abm_startup = 0;          // ABM3 start-up steps done (0..3)
     double abm_last_dt = 0.0;     // dt of the last ABM3 step
     void *hex = nullptr, *heff = nullptr;

@@ -41,6 +41,9 @@ bool backend_preview_f32(Backend &b, fullmag_fdm_observable o, uint32_t pnx, uin
 bool backend_snapshot_begin(Backend &b, fullmag_fdm_observable obs, Snapshot &s);
 void snapshot_free(Snapshot &s);
 void backend_free(Backend &b);
+bool backend_adjoint_forward(Backend &b, double dt, uint32_t n, uint32_t K, fullmag_fdm_step_stats *st);
+bool backend_adjoint_backward(Backend &b, const double *lam_soa, double *gms, double *ghext, double *ghac,
+                              double *lam0_soa);
 void prof_collect(Backend &b);
 
 }  // namespace fm

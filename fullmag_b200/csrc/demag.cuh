@@ -39,6 +39,7 @@ struct DemagArgs {
     const double *ms_map;   // may be null (then ms)
     double ms;
     const double *vf;       // boundary tiers: volume fraction (M = phi Ms m), else null
+    int unit_source;        // 1: source = m on active cells (the adjoint's -N * lambda)
     T *hd;                  // SoA demag field out
     double norm;            // 1 / (Lx Ly Lz)
     int lines_x;            // complex lines (= 2 rows) per x-pass block
@@ -59,7 +60,8 @@ template <typename T>
 __device__ __forceinline__ T demag_source(const DemagArgs<T> &a, long long i, T m) {
     if (a.vf) return (T)((a.vf[i] * a.ms) * (double)m);
     double msi;
-    return cell_active(a, i, msi) ? (T)((double)m * msi) : T(0);
+    if (!cell_active(a, i, msi)) return T(0);
+    return a.unit_source ? m : (T)((double)m * msi);
 }
 
 // Apply H = -N(k) M(k) for one frequency (kx, ky, kz); M is overwritten by H.

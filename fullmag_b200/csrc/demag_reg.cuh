@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
     const long long rowa = ((long long)z * ny + ya) * nx, rowb = rowa + nx;
     C *line = region + q * TE;
     // M = Ms m in the storage precision (Ms of the uniform material is exact in FP32)
-    const T msT = (T)a.ms;
+    const T msT = a.unit_source ? T(1) : (T)a.ms;
     auto in = [&](int j) -> C {
         C v = mk<T>(0, 0);
         if (!a.mask && !a.ms_map && !a.vf) {

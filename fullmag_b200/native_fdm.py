@@ -124,6 +124,7 @@ EXT_FUNCTIONS = (
     "fullmag_fdm_backend_profile_entry", "fullmag_fdm_backend_profile_reset",
     "fullmag_fdm_backend_memory_info", "fullmag_fdm_newell_spectra",
     "fullmag_fdm_backend_get_stream", "fullmag_fdm_random_unit_vectors",
+    "fullmag_fdm_adjoint_forward", "fullmag_fdm_adjoint_backward",
 )
 
 _lib = None
@@ -179,6 +180,8 @@ def load_library(build_if_missing: bool = True):
     L.fullmag_fdm_backend_get_stream.argtypes = [vp, C.POINTER(C.c_void_p)]
     L.fullmag_fdm_random_unit_vectors.argtypes = [C.c_uint64, C.c_uint64, _dp]
     L.fullmag_fdm_random_unit_vectors.restype = None
+    L.fullmag_fdm_adjoint_forward.argtypes = [vp, C.c_double, C.c_uint32, C.c_uint32, C.POINTER(StepStats)]
+    L.fullmag_fdm_adjoint_backward.argtypes = [vp, _dp, C.c_uint64, _dp, _dp, _dp, _dp]
     _lib = L
     return L
 
@@ -410,6 +413,28 @@ class NativeFdmBackend:
         st = StepStats()
         self._check(self._lib.fullmag_fdm_backend_step_n(self._h, dt, n, C.byref(st)), "step_n")
         return st.as_dict()
+
+    # -- adjoint of a Heun trajectory (fullmag_fdm_ext.h) --
+    def adjoint_forward(self, dt: float, n: int, checkpoint_every: int = 0) -> dict:
+        """n Heun steps from the current state, keeping device checkpoints
+        every `checkpoint_every` steps (0: ceil(sqrt(n)))."""
+        st = StepStats()
+        self._check(self._lib.fullmag_fdm_adjoint_forward(self._h, dt, n, checkpoint_every, C.byref(st)),
+                    "adjoint_forward")
+        return st.as_dict()
+
+    def adjoint_backward(self, dl_dm: np.ndarray) -> dict:
+        """dL/dm at the final state (AoS 3N) -> dL/dMs per cell, dL/dH_ext (3,),
+        dL/dH_ac (3,) in A/m, and dL/dm0 (AoS 3N)."""
+        g = np.ascontiguousarray(dl_dm, dtype=np.float64).reshape(-1)
+        gms = np.zeros(self.n)
+        ge = np.zeros(3)
+        ga = np.zeros(3)
+        g0 = np.zeros(3 * self.n)
+        self._check(self._lib.fullmag_fdm_adjoint_backward(
+            self._h, g.ctypes.data_as(_dp), g.size, gms.ctypes.data_as(_dp), ge.ctypes.data_as(_dp),
+            ga.ctypes.data_as(_dp), g0.ctypes.data_as(_dp)), "adjoint_backward")
+        return {"dl_dms": gms, "dl_dh_ext": ge, "dl_dh_ac": ga, "dl_dm0": g0}
 
     # -- transfers --
     def copy_field(self, observable: int, dtype=np.float64) -> np.ndarray:

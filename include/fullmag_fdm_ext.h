@@ -51,6 +51,31 @@ fullmag_fdm_backend *fullmag_fdm_backend_create_ext(const fullmag_fdm_plan_desc 
 int fullmag_fdm_backend_step_n(fullmag_fdm_backend *handle, double dt_seconds,
                                uint32_t n_steps, fullmag_fdm_step_stats *out_last);
 
+/* ---- Adjoint of a Heun trajectory (no counterpart in the reference) ----
+ *
+ * fullmag_fdm_adjoint_forward: from the current state, take n_steps Heun
+ * steps of dt exactly like n_steps calls of fullmag_fdm_backend_step, keeping
+ * the state every checkpoint_every steps on the device (0: ceil(sqrt(n_steps))).
+ * out_last receives the last step's stats.
+ *
+ * fullmag_fdm_adjoint_backward: with dl_dm = dL/dm at the final state (AoS,
+ * len = 3 * cell_count), replay each checkpoint segment and pull the cotangent
+ * back through the discrete Heun steps (exchange, demag, Zeeman and LLG).
+ * Outputs, each optional (NULL):
+ *   dl_dms     [cell_count]   dL/dMs per cell (sum it for a uniform Ms);
+ *   dl_dh_ext  [3]            dL/dH_ext, A/m (the static external field);
+ *   dl_dh_ac   [3]            dL/dH_ac, A/m (amplitude of H_ac sin(2 pi f t));
+ *   dl_dm0     [3 cell_count] dL/dm at the starting state (AoS).
+ * The backend is left at the final state.  Requires the Heun integrator and a
+ * plan without region exchange tables or boundary tiers; the backward pass
+ * must follow the forward pass with no step or upload in between.  Memory:
+ * (checkpoints + checkpoint_every + 10) state vectors in the plan's precision
+ * plus 7 FP64 vectors, allocated by the forward pass. */
+int fullmag_fdm_adjoint_forward(fullmag_fdm_backend *handle, double dt_seconds, uint32_t n_steps,
+                                uint32_t checkpoint_every, fullmag_fdm_step_stats *out_last);
+int fullmag_fdm_adjoint_backward(fullmag_fdm_backend *handle, const double *dl_dm, uint64_t len,
+                                 double *dl_dms, double *dl_dh_ext, double *dl_dh_ac, double *dl_dm0);
+
 /* Per-kernel device timing with CUDA events on the library's stream. */
 int fullmag_fdm_backend_set_profiling(fullmag_fdm_backend *handle, int enable);
 int fullmag_fdm_backend_profile_count(fullmag_fdm_backend *handle);
