@@ -23,15 +23,16 @@ template <int L1, int L2> __host__ __device__ constexpr int line_region() {
 // x forward: pack Ms*m (two rows per complex line), R2C, transposed store.
 // block = lines_x line groups of L2 threads; grid (ceil(ny / 2 lines_x), nz, 3)
 // ---------------------------------------------------------------------------
+// Block body (bx, z, c); also run per work item by the batched kernels
+// (batch.cuh), with the padded length Lx >= 2 nx.
 template <typename T, int L1, int L2>
-__global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
+__device__ __forceinline__ void xf_body(const DemagArgs<T> &a, int bx, int z, int c, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = line_region<L1, L2>();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *region = tw + L;
     const int LP = a.lines_x, RB = 2 * LP;
-    const int c = blockIdx.z, z = blockIdx.y, y0 = blockIdx.x * RB;
+    const int y0 = bx * RB;
     fill_tw4<L1, L2>(tw, a.twx, 1);
     __syncthreads();
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;
@@ -43,6 +44,7 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
     const T msT = a.unit_source ? T(1) : (T)a.ms;
     auto in = [&](int j) -> C {
         C v = mk<T>(0, 0);
+        if (j >= nx) return v;  // zero padding beyond the row (Lx > 2 nx)
         if (!a.mask && !a.ms_map && !a.vf) {
             if (ya < ny) v.x = mc[rowa + j] * msT;
             if (yb < ny) v.y = mc[rowb + j] * msT;
@@ -77,19 +79,24 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
     }
 }
 
+template <typename T, int L1, int L2>
+__global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    xf_body<T, L1, L2>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // x inverse: gather A/B half spectra (transposed), form Z = A + iB on the full
 // circle, C2R, crop, 1/P, mask.  Same grid as k_xf_r.
 // ---------------------------------------------------------------------------
 template <typename T, int L1, int L2>
-__global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
+__device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, int c, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = line_region<L1, L2>();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *region = tw + L;
     const int LP = a.lines_x, RB = 2 * LP, nx = a.nx, ny = a.ny, nkx = a.nkx;
-    const int c = blockIdx.z, z = blockIdx.y, y0 = blockIdx.x * RB;
+    const int y0 = bx * RB;
     fill_tw4<L1, L2>(tw, a.twx, 1);
     // Z[k] = A[k] + i B[k] (k <= nx), Z[L-k] = conj(A[k]) + i conj(B[k]); DC and
     // Nyquist taken as real.  Row pairs (A, B) sit in adjacent lanes.
@@ -100,7 +107,7 @@ __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
         if (ok && (r & 1) == 0) {
             C A = v, B = mk<T>(bx, by);
             C *ln = region + (r >> 1) * TE;
-            if (k == 0 || k == nx) {
+            if (k == 0 || k == L / 2) {
                 ln[k] = mk<T>(A.x, B.x);
             } else {
                 ln[k] = mk<T>(A.x - B.y, A.y + B.x);
@@ -157,48 +164,64 @@ __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
     fft4step<L1, L2, true, true, false>(t, tw, line, in, out);
 }
 
+template <typename T, int L1, int L2>
+__global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    xi_body<T, L1, L2>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // y forward (3-D): S1 -> S2, line g = (c, z, kx); block = lines_y groups of L2
 // ---------------------------------------------------------------------------
 template <typename T, int L1, int L2>
-__global__ void __launch_bounds__(256) k_yf_r(DemagArgs<T> a) {
+__device__ __forceinline__ void yf_body(const DemagArgs<T> &a, int bx, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = tile_elems(L1, L2);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *region = tw + L;
     fill_tw4<L1, L2>(tw, a.twy, 1);
     __syncthreads();
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2, ny = a.ny;
     const long long total = 3LL * a.nz * a.nkx;
-    const long long g = (long long)blockIdx.x * a.lines_y + q;
+    const long long g = (long long)bx * a.lines_y + q;
     const bool valid = g < total;
     const C *src = a.s1 + g * ny;
     C *dst = a.s2 + g * L;
-    auto in = [&](int j) -> C { return valid ? src[j] : mk<T>(0, 0); };
+    auto in = [&](int j) -> C { return (valid && j < ny) ? src[j] : mk<T>(0, 0); };
     auto out = [&](int k, C v) { if (valid) dst[k] = v; };
     fft4step<L1, L2, false, false, false, true>(t, tw, region + q * TE, in, out);
 }
 
+template <typename T, int L1, int L2>
+__global__ void __launch_bounds__(256) k_yf_r(DemagArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    yf_body<T, L1, L2>(a, blockIdx.x, smem_raw);
+}
+
 // y inverse (3-D): S2 -> S1, keeps y < ny
 template <typename T, int L1, int L2>
-__global__ void __launch_bounds__(256) k_yi_r(DemagArgs<T> a) {
+__device__ __forceinline__ void yi_body(const DemagArgs<T> &a, int bx, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = tile_elems(L1, L2);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *region = tw + L;
     fill_tw4<L1, L2>(tw, a.twy, 1);
     __syncthreads();
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2, ny = a.ny;
     const long long total = 3LL * a.nz * a.nkx;
-    const long long g = (long long)blockIdx.x * a.lines_y + q;
+    const long long g = (long long)bx * a.lines_y + q;
     const bool valid = g < total;
     const C *src = a.s2 + g * L;
     C *dst = a.s1 + g * ny;
     auto in = [&](int j) -> C { return valid ? src[j] : mk<T>(0, 0); };
     auto out = [&](int k, C v) { if (valid && k < ny) dst[k] = v; };
     fft4step<L1, L2, true, false, false>(t, tw, region + q * TE, in, out);
+}
+
+template <typename T, int L1, int L2>
+__global__ void __launch_bounds__(256) k_yi_r(DemagArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    yi_body<T, L1, L2>(a, blockIdx.x, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -211,8 +234,10 @@ __global__ void __launch_bounds__(256) k_yi_r(DemagArgs<T> a) {
 // so each thread of the pair holds 3 x nz values and the two halves are summed
 // with one shuffle exchange.
 // ---------------------------------------------------------------------------
+// One column task tid (tid / P = column, tid % P = kz parity); the task index
+// of a warp's lanes must be contiguous and start at a multiple of 32.
 template <typename T, int LZ, int P>
-__global__ void __launch_bounds__(128) k_zc_r(DemagArgs<T> a) {
+__device__ __forceinline__ void zc_task(const DemagArgs<T> &a, int tid) {
     using C = cx<T>;
     constexpr int NZL = LZ / P;  // points per thread
     static_assert(P == 1 || P == 2, "z split");
@@ -221,9 +246,8 @@ __global__ void __launch_bounds__(128) k_zc_r(DemagArgs<T> a) {
     const int nz = a.nz, Ly = a.Ly, nkx = a.nkx;
     const long long cs = (long long)nz * nkx * Ly;  // component stride in S2
     const long long zs = (long long)nkx * Ly;
-    const int h = (P == 2) ? (threadIdx.x & 1) : 0;
-    const int span = ((cols * P + 127) / 128) * 128;  // whole pairs and warps iterate together
-    for (int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < span; tid += gridDim.x * blockDim.x) {
+    const int h = (P == 2) ? (tid & 1) : 0;
+    {
         const int col = tid / P;
         const bool valid = col < cols;
         const int kx = valid ? col / Ly : 0;
@@ -293,6 +317,13 @@ __global__ void __launch_bounds__(128) k_zc_r(DemagArgs<T> a) {
             }
         }
     }
+}
+
+template <typename T, int LZ, int P>
+__global__ void __launch_bounds__(128) k_zc_r(DemagArgs<T> a) {
+    const int span = ((a.nkx * a.Ly * P + 127) / 128) * 128;  // whole pairs and warps iterate together
+    for (int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < span; tid += gridDim.x * blockDim.x)
+        zc_task<T, LZ, P>(a, tid);
 }
 
 // ---------------------------------------------------------------------------

@@ -157,13 +157,15 @@ struct HostFft {
     }
 };
 
-// In-place per-axis even/odd transform of lines of length n (stride s) into
-// n + 1 outputs (dst stride s2); L = 2 n.
-void axis_transform(const double *src, double *dst, size_t n, bool odd, const HostFft &fft) {
-    std::vector<std::complex<double>> buf(2 * n, 0.0);
+// Per-axis even/odd transform of a line of n samples f(0..n-1), extended to
+// the padded length L >= 2n with f(L - r) = +-f(r) and zeros between, into the
+// L/2 + 1 outputs k = 0..L/2: 2 Re F - f(0) (even) or -2 Im F (odd), F the
+// length-L DFT of f(0..n-1) followed by zeros.
+void axis_transform(const double *src, double *dst, size_t n, size_t L, bool odd, const HostFft &fft) {
+    std::vector<std::complex<double>> buf(L, 0.0);
     for (size_t x = 0; x < n; ++x) buf[x] = src[x];
     fft.run(buf.data());
-    for (size_t k = 0; k <= n; ++k)
+    for (size_t k = 0; k <= L / 2; ++k)
         dst[k] = odd ? -2.0 * buf[k].imag() : 2.0 * buf[k].real() - src[0];
 }
 
@@ -217,19 +219,24 @@ void newell_real_octant(int nx, int ny, int nz, double dx, double dy, double dz,
 
 void newell_octant_spectra(int nx, int ny, int nz, double dx, double dy, double dz, bool thin,
                            std::vector<double> (&spec)[6]) {
+    newell_octant_spectra_padded(nx, ny, nz, dx, dy, dz, thin, 2 * nx, 2 * ny, 2 * nz, spec);
+}
+
+void newell_octant_spectra_padded(int nx, int ny, int nz, double dx, double dy, double dz, bool thin,
+                                  int Lx, int Ly, int Lz, std::vector<double> (&spec)[6]) {
     std::vector<double> real[6];
     newell_real_octant(nx, ny, nz, dx, dy, dz, real);
-    const int KX = nx + 1, KY = ny + 1, KZ = thin ? 1 : nz + 1;
+    const int KX = Lx / 2 + 1, KY = Ly / 2 + 1, KZ = thin ? 1 : Lz / 2 + 1;
     // parity per component along (x, y, z): xx, yy, zz even; xy odd x,y; xz odd x,z; yz odd y,z
     const bool oddx[6] = {false, false, false, true, true, false};
     const bool oddy[6] = {false, false, false, true, false, true};
     const bool oddz[6] = {false, false, false, false, true, true};
-    HostFft fx(2 * (size_t)nx), fy(2 * (size_t)ny), fz(2 * (size_t)nz);
+    HostFft fx((size_t)Lx), fy((size_t)Ly), fz((size_t)(thin ? 2 * nz : Lz));
     for (int c = 0; c < 6; ++c) {
         // x: [z][y][x<nx] -> A[z][y][kx<=nx]
         std::vector<double> A((size_t)nz * ny * KX);
         parallel_for((size_t)nz * ny, [&](size_t line) {
-            axis_transform(&real[c][line * nx], &A[line * KX], nx, oddx[c], fx);
+            axis_transform(&real[c][line * nx], &A[line * KX], nx, Lx, oddx[c], fx);
         });
         // y: A[z][y][kx] -> B[z][kx][ky<=ny]
         std::vector<double> B((size_t)nz * KX * KY);
@@ -237,7 +244,7 @@ void newell_octant_spectra(int nx, int ny, int nz, double dx, double dy, double 
             const size_t z = line / KX, kx = line % KX;
             std::vector<double> src(ny), dst(KY);
             for (int y = 0; y < ny; ++y) src[y] = A[(z * ny + y) * KX + kx];
-            axis_transform(src.data(), dst.data(), ny, oddy[c], fy);
+            axis_transform(src.data(), dst.data(), ny, Ly, oddy[c], fy);
             for (int ky = 0; ky < KY; ++ky) B[(z * KX + kx) * KY + ky] = dst[ky];
         });
         // z: B[z][kx][ky] -> spec[kz][kx][ky]; thin films keep only the z = 0 plane
@@ -255,7 +262,7 @@ void newell_octant_spectra(int nx, int ny, int nz, double dx, double dy, double 
         parallel_for((size_t)KX * KY, [&](size_t line) {
             std::vector<double> src(nz), dst(KZ);
             for (int z = 0; z < nz; ++z) src[z] = B[(size_t)z * KX * KY + line];
-            axis_transform(src.data(), dst.data(), nz, oddz[c], fz);
+            axis_transform(src.data(), dst.data(), nz, Lz, oddz[c], fz);
             for (int kz = 0; kz < KZ; ++kz) spec[c][(size_t)kz * KX * KY + line] = sign * dst[kz];
         });
     }

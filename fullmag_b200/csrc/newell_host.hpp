@@ -15,4 +15,10 @@ void newell_real_octant(int nx, int ny, int nz, double dx, double dy, double dz,
 void newell_octant_spectra(int nx, int ny, int nz, double dx, double dy, double dz, bool thin,
                            std::vector<double> (&spec)[6]);
 
+// The same for padded lengths L >= 2n per axis (even): octant kx <= Lx/2,
+// ky <= Ly/2, kz <= Lz/2.  Outputs at the physical cells use only kernel offsets
+// |r| <= n - 1, so any such L gives the field of L = 2n in exact arithmetic.
+void newell_octant_spectra_padded(int nx, int ny, int nz, double dx, double dy, double dz, bool thin,
+                                  int Lx, int Ly, int Lz, std::vector<double> (&spec)[6]);
+
 }  // namespace fm

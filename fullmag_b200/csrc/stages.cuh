@@ -407,17 +407,17 @@ struct PlaneLoads {
     T hd[3];   // H_d(x, y, z)
 };
 
+// Block body (bx, by, bz); the diagnostics accumulate into acc.  Also run per
+// work item by the batched kernels (batch.cuh).
 template <typename T, int MODE>
-__global__ void __launch_bounds__(128, 4) k_stage_plain(StageArgs<T> a, int zb) {
+__device__ __forceinline__ void stage_plain_body(const StageArgs<T> &a, int zb, int bx, int by, int bz,
+                                                 double (&acc)[NQ]) {
     using R = double;
-    double acc[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const unsigned n = (unsigned)a.n, sxy = (unsigned)nx * (unsigned)ny;
     const int lane = threadIdx.x;
-    const int x = blockIdx.x * 32 + lane, y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z0 = blockIdx.z * zb, z1 = min(z0 + zb, nz);
+    const int x = bx * 32 + lane, y = by * blockDim.y + threadIdx.y;
+    const int z0 = bz * zb, z1 = min(z0 + zb, nz);
     const bool inxy = x < nx && y < ny;
     const int xc = min(x, nx - 1), yc = min(y, ny - 1);
     const T *f0 = a.m, *f1 = a.m + n, *f2 = a.m + 2 * (size_t)n;
@@ -557,6 +557,14 @@ __global__ void __launch_bounds__(128, 4) k_stage_plain(StageArgs<T> a, int zb) 
         }
         L = Ln;
     }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(128, 4) k_stage_plain(StageArgs<T> a, int zb) {
+    double acc[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+    stage_plain_body<T, MODE>(a, zb, blockIdx.x, blockIdx.y, blockIdx.z, acc);
     if (a.partials) block_reduce_final(acc, a.partials, a.counter, a.out);
 }
 
@@ -581,10 +589,9 @@ struct CombineArgs {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_combine(CombineArgs<T> a) {
+__device__ __forceinline__ void combine_cell(const CombineArgs<T> &a, long long i) {
     const long long n = a.n;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    {
         double v[3];
 #pragma unroll
         for (int comp = 0; comp < 3; ++comp) {
@@ -621,6 +628,13 @@ __global__ void __launch_bounds__(256) k_combine(CombineArgs<T> a) {
         a.out[n + i] = (T)(v[1] * inv);
         a.out[2 * n + i] = (T)(v[2] * inv);
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_combine(CombineArgs<T> a) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+         i += (long long)gridDim.x * blockDim.x)
+        combine_cell(a, i);
 }
 
 }  // namespace fm

@@ -125,7 +125,21 @@ EXT_FUNCTIONS = (
     "fullmag_fdm_backend_memory_info", "fullmag_fdm_newell_spectra",
     "fullmag_fdm_backend_get_stream", "fullmag_fdm_random_unit_vectors",
     "fullmag_fdm_adjoint_forward", "fullmag_fdm_adjoint_backward",
+    "fullmag_fdm_batch_create", "fullmag_fdm_batch_step_n", "fullmag_fdm_batch_copy_m",
+    "fullmag_fdm_batch_tuning", "fullmag_fdm_batch_last_error", "fullmag_fdm_batch_destroy",
 )
+
+class BatchProblem(C.Structure):
+    """fullmag_fdm_batch_problem (include/fullmag_fdm_ext.h)."""
+    _fields_ = [
+        ("nx", C.c_uint32), ("ny", C.c_uint32), ("nz", C.c_uint32),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+        ("saturation_magnetisation", C.c_double), ("exchange_stiffness", C.c_double),
+        ("damping", C.c_double), ("gyromagnetic_ratio", C.c_double),
+        ("external_field_am", C.c_double * 3),
+        ("initial_magnetization_xyz", _dp),
+    ]
+
 
 _lib = None
 
@@ -182,6 +196,15 @@ def load_library(build_if_missing: bool = True):
     L.fullmag_fdm_random_unit_vectors.restype = None
     L.fullmag_fdm_adjoint_forward.argtypes = [vp, C.c_double, C.c_uint32, C.c_uint32, C.POINTER(StepStats)]
     L.fullmag_fdm_adjoint_backward.argtypes = [vp, _dp, C.c_uint64, _dp, _dp, _dp, _dp]
+    L.fullmag_fdm_batch_create.restype = vp
+    L.fullmag_fdm_batch_create.argtypes = [C.POINTER(BatchProblem), C.c_uint32, C.c_int]
+    L.fullmag_fdm_batch_step_n.argtypes = [vp, C.c_double, C.c_uint32]
+    L.fullmag_fdm_batch_copy_m.argtypes = [vp, C.c_uint32, _dp, C.c_uint64]
+    L.fullmag_fdm_batch_tuning.argtypes = [vp, C.POINTER(C.c_int32), C.c_uint32]
+    L.fullmag_fdm_batch_last_error.restype = C.c_char_p
+    L.fullmag_fdm_batch_last_error.argtypes = [vp]
+    L.fullmag_fdm_batch_destroy.argtypes = [vp]
+    L.fullmag_fdm_batch_destroy.restype = None
     _lib = L
     return L
 
@@ -524,3 +547,71 @@ class NativeFdmBackend:
         dims = (C.c_uint32 * 3)()
         self._lib.fullmag_fdm_backend_memory_info(self._h, C.byref(b), dims)
         return b.value, tuple(dims)
+
+
+class NativeFdmBatch:
+    """Many independent uniform-material problems stepped together with Heun
+    (fullmag_fdm_batch_*).  `problems` is a list of dicts with keys cells,
+    cell_size, ms, aex, alpha, gamma, h_ext (A/m) and m0 (AoS 3N)."""
+
+    def __init__(self, problems, precision: int = PRECISION_SINGLE):
+        self._lib = load_library()
+        arr = (BatchProblem * len(problems))()
+        self._keep = []
+        self.sizes = []
+        for i, p in enumerate(problems):
+            nx, ny, nz = (int(v) for v in p["cells"])
+            b = arr[i]
+            b.nx, b.ny, b.nz = nx, ny, nz
+            b.dx, b.dy, b.dz = (float(v) for v in p["cell_size"])
+            b.saturation_magnetisation = float(p["ms"])
+            b.exchange_stiffness = float(p["aex"])
+            b.damping = float(p["alpha"])
+            b.gyromagnetic_ratio = float(p.get("gamma", 2.211e5))
+            for c, v in enumerate(p.get("h_ext", (0.0, 0.0, 0.0))):
+                b.external_field_am[c] = float(v)
+            m0 = np.ascontiguousarray(p["m0"], dtype=np.float64).reshape(-1)
+            assert m0.size == 3 * nx * ny * nz
+            self._keep.append(m0)
+            b.initial_magnetization_xyz = m0.ctypes.data_as(_dp)
+            self.sizes.append(nx * ny * nz)
+        self._h = self._lib.fullmag_fdm_batch_create(arr, len(problems), precision)
+        if not self._h:
+            raise RunError("fullmag_fdm_batch_create returned NULL")
+        err = self._lib.fullmag_fdm_batch_last_error(self._h)
+        if err:
+            self.close()
+            raise RunError(err.decode())
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            err = self._lib.fullmag_fdm_batch_last_error(self._h)
+            raise RunError(f"{what}: {err.decode() if err else rc}")
+
+    def step_n(self, dt: float, n: int) -> None:
+        self._check(self._lib.fullmag_fdm_batch_step_n(self._h, dt, n), "batch_step_n")
+
+    def copy_m(self, index: int) -> np.ndarray:
+        out = np.zeros(3 * self.sizes[index])
+        self._check(self._lib.fullmag_fdm_batch_copy_m(self._h, index, out.ctypes.data_as(_dp), out.size),
+                    "batch_copy_m")
+        return out
+
+    def tuning(self):
+        g = (C.c_int32 * 7)()
+        self._check(self._lib.fullmag_fdm_batch_tuning(self._h, g, 7), "batch_tuning")
+        return list(g)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.fullmag_fdm_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()

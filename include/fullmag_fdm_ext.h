@@ -76,6 +76,39 @@ int fullmag_fdm_adjoint_forward(fullmag_fdm_backend *handle, double dt_seconds, 
 int fullmag_fdm_adjoint_backward(fullmag_fdm_backend *handle, const double *dl_dm, uint64_t len,
                                  double *dl_dms, double *dl_dh_ext, double *dl_dh_ac, double *dl_dm0);
 
+/* ---- Batched ensemble (no counterpart in the reference) ----
+ *
+ * Many independent uniform-material problems (own grid, cell size, Ms, A,
+ * alpha, gamma, static field and m0) stepped together with Heun: every stage
+ * of a step is one persistent launch over all problems, and a step is one
+ * CUDA graph.  Grids up to 512 x 512 x 8 cells; the demag spectra are the
+ * library's FP64 Newell tensor (no mask, regions or boundary tiers).  On the
+ * first fullmag_fdm_batch_step_n call an autotuner picks each kernel's
+ * persistent grid size; fullmag_fdm_batch_tuning reports the picks (7 values:
+ * x forward, y forward, z convolution, y inverse, x inverse, stage, predictor).
+ * create returns a handle even on failure, with last_error set (NULL only when
+ * the handle itself cannot be allocated). */
+typedef struct {
+    uint32_t nx, ny, nz;
+    double dx, dy, dz;
+    double saturation_magnetisation;
+    double exchange_stiffness;
+    double damping;
+    double gyromagnetic_ratio;
+    double external_field_am[3];
+    const double *initial_magnetization_xyz; /* AoS, 3 nx ny nz; read during create */
+} fullmag_fdm_batch_problem;
+
+typedef struct fullmag_fdm_batch fullmag_fdm_batch;
+
+fullmag_fdm_batch *fullmag_fdm_batch_create(const fullmag_fdm_batch_problem *problems, uint32_t count,
+                                            fullmag_fdm_precision precision);
+int fullmag_fdm_batch_step_n(fullmag_fdm_batch *batch, double dt_seconds, uint32_t n_steps);
+int fullmag_fdm_batch_copy_m(fullmag_fdm_batch *batch, uint32_t index, double *out_xyz, uint64_t len);
+int fullmag_fdm_batch_tuning(const fullmag_fdm_batch *batch, int32_t *grid_sizes, uint32_t len);
+const char *fullmag_fdm_batch_last_error(const fullmag_fdm_batch *batch);
+void fullmag_fdm_batch_destroy(fullmag_fdm_batch *batch);
+
 /* Per-kernel device timing with CUDA events on the library's stream. */
 int fullmag_fdm_backend_set_profiling(fullmag_fdm_backend *handle, int enable);
 int fullmag_fdm_backend_profile_count(fullmag_fdm_backend *handle);
