@@ -149,6 +149,7 @@ struct Impl {
         a.KZ = b.KZ; a.KY = b.KY;
         a.px = b.px; a.py = b.py; a.pz = b.pz;
         a.twx = (const C *)b.twx; a.twy = (const C *)b.twy; a.twz = (const C *)b.twz;
+        a.twxT = (const C *)b.twxT; a.twyT = (const C *)b.twyT;
         a.s1 = (C *)b.s1; a.s2 = (C *)b.s2;
         a.spec = (const T *)b.spec;
         a.m = (const T *)m;
@@ -181,10 +182,10 @@ struct Impl {
                 const int unit = L2 >= 32 ? 1 : 32 / L2;    // lines per warp multiple
                 int lp = std::max(1, target / L2);
                 lp = std::min(lp, std::max(unit, ((b.ny + 1) / 2 + unit - 1) / unit * unit));
-                while (lp > unit && (size_t)(L1 * L2 + lp * TE) * sz > maxs) lp -= unit;
+                while (lp > unit && (size_t)(lp * TE) * sz > maxs) lp -= unit;
                 b.lines_x = lp;
                 b.thr_x = lp * L2;
-                b.rsm_x = (size_t)(L1 * L2 + lp * TE) * sz;
+                b.rsm_x = (size_t)(lp * TE) * sz;
                 ok &= cuda_ok(b, cudaFuncSetAttribute(k_xf_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_x), "attr xf_r");
                 ok &= cuda_ok(b, cudaFuncSetAttribute(k_xi_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_x), "attr xi_r");
             }
@@ -198,10 +199,10 @@ struct Impl {
                     const int unit = L2 >= 32 ? 1 : 32 / L2;  // kb multiple so 3*kb*L2 % 32 == 0
                     int kb = std::max(unit, (256 / (3 * L2)) / unit * unit);
                     kb = std::min(kb, std::max(unit, (b.nkx + unit - 1) / unit * unit));
-                    while (kb > unit && (size_t)(L1 * L2 + 3 * kb * TE) * sz > maxs) kb -= unit;
+                    while (kb > unit && (size_t)(3 * kb * TE) * sz > maxs) kb -= unit;
                     b.kb_y = kb;
                     b.thr_yc = 3 * kb * L2;
-                    b.rsm_yc = (size_t)(L1 * L2 + 3 * kb * TE) * sz;
+                    b.rsm_yc = (size_t)(3 * kb * TE) * sz;
                     ok &= b.rsm_yc <= 227 * 1024 && b.thr_yc <= 256;
                     ok &= cuda_ok(b, cudaFuncSetAttribute(k_yc_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_yc), "attr yc_r");
                 } else {
@@ -209,7 +210,7 @@ struct Impl {
                     const int lpb = std::max(1, 256 / L2);
                     b.lines_y = lpb;
                     b.thr_y = lpb * L2;
-                    b.rsm_y = (size_t)(L1 * L2 + lpb * TE) * sz;
+                    b.rsm_y = (size_t)(lpb * TE) * sz;
                     ok &= cuda_ok(b, cudaFuncSetAttribute(k_yf_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_y), "attr yf_r");
                     ok &= cuda_ok(b, cudaFuncSetAttribute(k_yi_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_y), "attr yi_r");
                 }
@@ -439,9 +440,12 @@ struct Impl {
     }
 
     // k = RHS(m, t); optional observables and diagnostics.
-    static bool eval(Backend &b, const void *m, double t, void *kout, bool diag, bool obs) {
+    static bool eval(Backend &b, const void *m, double t, void *kout, bool diag, bool obs,
+                     void *pred_out = nullptr, double pred_dt = 0.0) {
         StageArgs<T> s = stage_args(b, m, t);
         s.kout = (T *)kout;
+        s.pred_out = (T *)pred_out;
+        s.pred_dt = pred_dt;
         s.hex_out = obs ? (T *)b.hex : nullptr;
         s.heff_out = obs ? (T *)b.heff : nullptr;
         s.partials = diag ? b.partials : nullptr;
@@ -521,8 +525,10 @@ struct Impl {
     // One Heun step (lib.rs:1217-1249) with the cached k1.
     static bool heun(Backend &b, double dt, fullmag_fdm_step_stats *st, bool readback) {
         if (!ensure_k1(b)) return false;
-        // predictor m_p = normalize(m + k1 dt)
-        if (!combine(b, 0, b.m, {b.k[0]}, {dt}, dt, b.mstage)) return false;
+        // predictor m_p = normalize(m + k1 dt); the previous step's RHS kernel
+        // already wrote it when this dt equals the previous one
+        if (!(b.pred_valid && b.pred_dt == dt) && !combine(b, 0, b.m, {b.k[0]}, {dt}, dt, b.mstage)) return false;
+        b.pred_valid = false;
         if (!demag(b, b.mstage, b.hd)) return false;
         // corrector at m_p: k2 and m <- normalize(m0 + (k1 + k2) dt/2)
         StageArgs<T> s = stage_args(b, b.mstage, b.time + dt);
@@ -535,9 +541,11 @@ struct Impl {
             launch_stage<MODE_HEUN_CORR>(b, s);
         }
         if (!check_launch(b, "heun corrector")) return false;
-        // fields, RHS (next k1) and diagnostics at the new state
+        // fields, RHS (next k1), the next predictor and diagnostics at the new state
         if (!demag(b, b.m, b.hd)) return false;
-        if (!eval(b, b.m, b.time + dt, b.k[0], true, false)) return false;
+        if (!eval(b, b.m, b.time + dt, b.k[0], true, false, b.mstage, dt)) return false;
+        b.pred_valid = true;
+        b.pred_dt = dt;
         b.time += dt;
         b.step_count += 1;
         b.k1_valid = true;
@@ -552,6 +560,7 @@ struct Impl {
 
     // One accepted DP45 step (lib.rs:1412-1568).
     static bool dp45(Backend &b, double dt_in, fullmag_fdm_step_stats *st) {
+        b.pred_valid = false;  // the stages below use mstage
         const double A21 = 1.0 / 5.0;
         const double A31 = 3.0 / 40.0, A32 = 9.0 / 40.0;
         const double A41 = 44.0 / 45.0, A42 = -56.0 / 15.0, A43 = 32.0 / 9.0;
@@ -636,6 +645,7 @@ struct Impl {
     // One classical RK4 step (lib.rs:1253-1297) with the cached k1; stage
     // times t, t + dt/2, t + dt/2, t + dt.
     static bool rk4(Backend &b, double dt, fullmag_fdm_step_stats *st, bool readback) {
+        b.pred_valid = false;  // the stages below use mstage
         if (!ensure_k1(b)) return false;
         void **k = b.k;
         const double t = b.time;
@@ -656,6 +666,7 @@ struct Impl {
     // same values.  Stage times t, t + dt/2, t + 3dt/4, t + dt; k4 = RHS(y3) is
     // the next step's k1.
     static bool rk23(Backend &b, double dt_in, fullmag_fdm_step_stats *st) {
+        b.pred_valid = false;  // the stages below use mstage
         double dt = std::max(std::min(dt_in, b.dt_max), b.dt_min);
         if (!ensure_k1(b)) return false;
         void **k = b.k;
@@ -722,6 +733,7 @@ struct Impl {
         if (b.abm_last_dt > 0.0 && std::fabs(dt - b.abm_last_dt) / b.abm_last_dt > 0.1) b.abm_startup = 0;
         void **k = b.k;
         if (b.abm_startup < 3) {
+            if (b.abm_startup == 0) b.pred_valid = false;
             if (!heun(b, dt, st, readback)) return false;
             // heun() left RHS(m_{n+1}) in k[0]; the history keeps a copy
             if (!cuda_ok(b, cudaMemcpyAsync(k[1], k[0], (size_t)3 * b.n * sizeof(T), cudaMemcpyDeviceToDevice, b.stream),
@@ -731,6 +743,7 @@ struct Impl {
             return true;
         }
         const double t = b.time;
+        b.pred_valid = false;
         if (!combine(b, 2, b.m, {k[2], k[3], k[4]}, {23.0 / 12.0, -16.0 / 12.0, 5.0 / 12.0}, dt, b.mstage)) return false;
         if (!demag(b, b.mstage, b.hd) || !eval(b, b.mstage, t + dt, k[1], false, false)) return false;
         if (!combine(b, 2, b.m, {k[1], k[2], k[3]}, {5.0 / 12.0, 8.0 / 12.0, -1.0 / 12.0}, dt, b.m)) return false;
@@ -872,6 +885,7 @@ struct Impl {
             b.time = b.adj_ck_time[c];
             b.step_count = b.adj_ck_step[c];
             b.k1_valid = false;
+            b.pred_valid = false;
             for (uint32_t j = 0; ok && j < len; ++j) {
                 ok = cuda_ok(b, cudaMemcpyAsync(p.seg + (size_t)j * v, b.m, vb, cudaMemcpyDeviceToDevice, b.stream), "segment");
                 seg_time[j] = b.time;
@@ -885,6 +899,7 @@ struct Impl {
         b.time = b.adj_t_final;
         b.step_count = b.adj_step_final;
         b.k1_valid = false;
+        b.pred_valid = false;
         b.obs_valid = false;
         if (!ok) return false;
         if (gms_host && !cuda_ok(b, cudaMemcpyAsync(gms_host, p.gms, (size_t)b.n * 8, cudaMemcpyDeviceToHost, b.stream), "dL/dMs")) return false;
@@ -1002,6 +1017,8 @@ bool backend_alloc(Backend &b) {
     if (b.enable_demag) {
         items.push_back({&b.twx, (size_t)b.Lx * cs});
         items.push_back({&b.twy, (size_t)b.Ly * cs});
+        items.push_back({&b.twxT, (size_t)b.Lx * cs});
+        items.push_back({&b.twyT, (size_t)b.Ly * cs});
         items.push_back({&b.twz, (size_t)b.Lz * cs});
         items.push_back({&b.s1, (size_t)3 * b.nz * b.nkx * b.ny * cs});
         if (!b.thin) items.push_back({&b.s2, (size_t)3 * b.nz * b.nkx * b.Ly * cs});
@@ -1067,6 +1084,12 @@ static bool upload_tables(Backend &b, const std::vector<double> (&spec)[6]) {
         return cuda_ok(b, cudaMemcpy(dst, t.data(), L * sizeof(cx<T>), cudaMemcpyHostToDevice), "twiddles");
     };
     if (!tw(b.Lx, b.twx) || !tw(b.Ly, b.twy) || !tw(b.Lz, b.twz)) return false;
+    auto tw4 = [&](int L, void *dst) {
+        if (L < 2 || (L & (L - 1))) return true;  // register FFT only (powers of two)
+        const std::vector<cx<T>> t = host_tw4<T>(L);
+        return cuda_ok(b, cudaMemcpy(dst, t.data(), L * sizeof(cx<T>), cudaMemcpyHostToDevice), "twiddles (4-step)");
+    };
+    if (!tw4(b.Lx, b.twxT) || !tw4(b.Ly, b.twyT)) return false;
     const size_t plane = (size_t)b.KZ * b.nkx * b.KY;
     std::vector<T> host(6 * plane);
     for (int c = 0; c < 6; ++c)
@@ -1096,6 +1119,7 @@ static bool upload_m_impl(Backend &b, const TI *host, uint64_t len) {
         k_aos_to_soa<TI, float><<<cgrid(b.n), 256, 0, b.stream>>>((const TI *)b.staging, (float *)b.m, b.n, b.d_mask, b.d_msmap);
     if (!check_launch(b, "aos_to_soa")) return false;
     b.k1_valid = false;
+    b.pred_valid = false;
     b.obs_valid = false;
     return cuda_ok(b, cudaStreamSynchronize(b.stream), "upload sync");
 }

@@ -68,6 +68,8 @@ struct Backend {
     double adj_t_final = 0.0;
     uint64_t adj_step_final = 0;
     bool adj_ready = false;
+    bool pred_valid = false;      // mstage holds normalize(m + k1 pred_dt) (Heun's next predictor)
+    double pred_dt = 0.0;
     int abm_startup = 0;          // ABM3 start-up steps done (0..3)
     double abm_last_dt = 0.0;     // dt of the last ABM3 step
     void *hex = nullptr, *heff = nullptr;
@@ -83,6 +85,7 @@ struct Backend {
     int Lx = 0, Ly = 0, Lz = 0, nkx = 0, KZ = 0, KY = 0;
     LinePlan px{}, py{}, pz{};
     void *twx = nullptr, *twy = nullptr, *twz = nullptr;
+    void *twxT = nullptr, *twyT = nullptr;  // 4-step twiddle tables (fftreg.cuh fill_tw4 order)
     void *s1 = nullptr, *s2 = nullptr, *spec = nullptr;
     int lines_x = 1, lines_y = 1, kt_z = 1, kb_y = 1;
     size_t smem_xf = 0, smem_yf = 0, smem_z = 0, smem_yc = 0;

@@ -63,7 +63,8 @@ struct BatchImpl {
     };
     std::vector<Prob> probs;
     void *arena = nullptr;
-    std::vector<std::pair<int, size_t>> tw_off;  // (L, offset) of shared twiddle tables
+    std::vector<std::pair<int, size_t>> tw_off;   // (L, offset) of shared twiddle tables
+    std::vector<std::pair<int, size_t>> tw4_off;  // (L, offset) of the 4-step tables (host_tw4)
     // device argument tables and work lists
     DemagArgs<T> *dA_m = nullptr, *dA_s = nullptr;  // demag of m / of m_stage
     StageArgs<T> *dS_eval = nullptr, *dS_corr = nullptr;
@@ -132,7 +133,10 @@ struct BatchImpl {
             for (int L : Ls) {
                 bool have = false;
                 for (auto &t : tw_off) have = have || t.first == L;
-                if (!have) tw_off.push_back({L, take((size_t)L * cs)});
+                if (!have) {
+                    tw_off.push_back({L, take((size_t)L * cs)});
+                    tw4_off.push_back({L, take((size_t)L * cs)});
+                }
             }
         }
         // work lists
@@ -195,6 +199,11 @@ struct BatchImpl {
             if (!batch_ok(B, cudaMemcpy(base() + t.second, tw.data(), tw.size() * sizeof(C), cudaMemcpyHostToDevice), "upload twiddles"))
                 return false;
         }
+        for (auto &t : tw4_off) {
+            const std::vector<C> tw = host_tw4<T>(t.first);
+            if (!batch_ok(B, cudaMemcpy(base() + t.second, tw.data(), tw.size() * sizeof(C), cudaMemcpyHostToDevice), "upload 4-step twiddles"))
+                return false;
+        }
         // per problem: octant spectra, m0, shared-memory needs
         std::vector<int> zb(count);
         for (uint32_t i = 0; i < count; ++i) {
@@ -216,9 +225,9 @@ struct BatchImpl {
             zb[i] = (int)d.nz;
             const int lx2 = l2_of(p.Lx), ly2 = l2_of(p.Ly);
             const size_t TEx = (size_t)std::max(lx2 == 1 ? 0 : (p.Lx / lx2) * (lx2 + 1), p.Lx) + 1;
-            smem_x = std::max(smem_x, ((size_t)p.Lx + (size_t)(256 / lx2) * TEx) * cs);
+            smem_x = std::max(smem_x, ((size_t)(256 / lx2) * TEx) * cs);
             const size_t TEy = ly2 == 1 ? 0 : (size_t)(p.Ly / ly2) * (ly2 + 1);
-            smem_y = std::max(smem_y, ((size_t)p.Ly + (size_t)(256 / ly2) * TEy) * cs);
+            smem_y = std::max(smem_y, ((size_t)(256 / ly2) * TEy) * cs);
         }
         if (!batch_ok(B, cudaMemcpy(d_zb, zb.data(), count * sizeof(int), cudaMemcpyHostToDevice), "upload zb")) return false;
         if (smem_x > 227 * 1024 || smem_y > 227 * 1024) { B.last_error = "batch FFT tiles exceed shared memory"; return false; }
@@ -232,6 +241,12 @@ struct BatchImpl {
 
     const C *tw(int L) {
         for (auto &t : tw_off)
+            if (t.first == L) return (const C *)(base() + t.second);
+        return nullptr;
+    }
+
+    const C *tw4(int L) {
+        for (auto &t : tw4_off)
             if (t.first == L) return (const C *)(base() + t.second);
         return nullptr;
     }
@@ -253,6 +268,7 @@ struct BatchImpl {
             a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.n = p.n;
             a.Lx = p.Lx; a.Ly = p.Ly; a.Lz = p.Lz; a.nkx = p.nkx; a.KZ = p.KZ; a.KY = p.KY;
             a.twx = tw(p.Lx); a.twy = tw(p.Ly); a.twz = tw(p.Lz);
+            a.twxT = tw4(p.Lx); a.twyT = tw4(p.Ly);
             a.s1 = (C *)(base() + p.off_s1);
             a.s2 = (C *)(base() + p.off_s2);
             a.spec = (const T *)(base() + p.off_spec);
@@ -280,7 +296,10 @@ struct BatchImpl {
             s.hd = hd;
             s.m = m;
             s.kout = k1;
+            s.pred_out = ms;  // the next step's predictor, written by the RHS kernel
+            s.pred_dt = dt;
             hS_eval[i] = s;
+            s.pred_out = nullptr;
             s.m = ms;
             s.kout = nullptr;
             s.m0 = m;
@@ -357,9 +376,9 @@ struct BatchImpl {
         return batch_ok(B, cudaGetLastError(), "autotune launches");
     }
 
-    // one Heun step: predictor, demag(m_p), corrector, demag(m), RHS (next k1)
+    // one Heun step: demag(m_p), corrector, demag(m), RHS (next k1 and the next
+    // predictor m_p; the first one comes from the initial RHS launch)
     void step_launches(cudaStream_t st) {
-        launch(st, KCOMB, false, grid[KCOMB]);
         demag(st, true);
         launch(st, KSTAGE, true, grid[KSTAGE]);
         demag(st, false);
@@ -371,6 +390,7 @@ struct BatchImpl {
             if (!upload_args(B, dt)) return false;
             if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
             if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+            k1_valid = false;  // the stored predictor used the previous dt
         }
         if (!tuned && !tune(B)) return false;
         if (!k1_valid) {

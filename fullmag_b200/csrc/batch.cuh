@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(256) k_batch_x(const DemagArgs<T> *__restrict_
         switch (a.Lx) {
 #define FM_X(L1, L2)                                                             \
     if (INV) xi_body<T, L1, L2>(a, it.y, it.z, it.w, smem_raw);                  \
-    else xf_body<T, L1, L2>(a, it.y, it.z, it.w, smem_raw);                      \
+    else xf_body<T, L1, L2, true>(a, it.y, it.z, it.w, smem_raw);                \
     break;
             case 16: FM_X(16, 1)
             case 32: FM_X(32, 1)
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(256) k_batch_y(const DemagArgs<T> *__restrict_
         switch (a.Ly) {
 #define FM_Y(L1, L2)                                                             \
     if (INV) yi_body<T, L1, L2>(a, it.y, smem_raw);                              \
-    else yf_body<T, L1, L2>(a, it.y, smem_raw);                                  \
+    else yf_body<T, L1, L2, true>(a, it.y, smem_raw);                            \
     break;
             case 16: FM_Y(16, 1)
             case 32: FM_Y(32, 1)
@@ -79,10 +79,10 @@ __global__ void __launch_bounds__(128) k_batch_z(const DemagArgs<T> *__restrict_
         const DemagArgs<T> &a = A[it.x];
         const int tid = it.y * 128 + threadIdx.x;
         switch (a.Lz) {
-            case 2: zc_task<T, 2, 1>(a, tid); break;
-            case 4: zc_task<T, 4, 1>(a, tid); break;
-            case 8: zc_task<T, 8, 1>(a, tid); break;
-            case 16: zc_task<T, 16, 2>(a, tid); break;
+            case 2: zc_task<T, 2, 1>(a, tid, 0); break;
+            case 4: zc_task<T, 4, 1>(a, tid, 0); break;
+            case 8: zc_task<T, 8, 1>(a, tid, 0); break;
+            case 16: zc_task<T, 16, 2>(a, tid, threadIdx.x & 1); break;
             default: break;
         }
     }

@@ -32,6 +32,9 @@ struct DemagArgs {
     int KZ, KY;             // octant extents: kz in [0, KZ), ky in [0, KY)
     LinePlan px, py, pz;
     const cx<T> *twx, *twy, *twz;
+    // register-FFT inter-level twiddles in the order fft4step reads them
+    // (twT[k1 L2 + t] = W_L^{k1 t}, fill_tw4's layout), read from global memory
+    const cx<T> *twxT, *twyT;
     cx<T> *s1, *s2;
     const T *spec;          // octant, 6 components
     const T *m;             // SoA magnetisation, component stride n

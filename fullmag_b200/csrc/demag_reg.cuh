@@ -24,17 +24,16 @@ template <int L1, int L2> __host__ __device__ constexpr int line_region() {
 // block = lines_x line groups of L2 threads; grid (ceil(ny / 2 lines_x), nz, 3)
 // ---------------------------------------------------------------------------
 // Block body (bx, z, c); also run per work item by the batched kernels
-// (batch.cuh), with the padded length Lx >= 2 nx.
-template <typename T, int L1, int L2>
+// (batch.cuh).  PAD: the padded length may exceed 2 nx (batch), so inputs
+// j >= nx are zero; otherwise Lx = 2 nx and the half-input pruning covers them.
+template <typename T, int L1, int L2, bool PAD = false>
 __device__ __forceinline__ void xf_body(const DemagArgs<T> &a, int bx, int z, int c, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = line_region<L1, L2>();
-    C *tw = reinterpret_cast<C *>(smem_raw);
-    C *region = tw + L;
+    const C *tw = a.twxT;
+    C *region = reinterpret_cast<C *>(smem_raw);
     const int LP = a.lines_x, RB = 2 * LP;
     const int y0 = bx * RB;
-    fill_tw4<L1, L2>(tw, a.twx, 1);
-    __syncthreads();
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;
     const T *mc = a.m + (long long)c * a.n;
     const int ya = y0 + 2 * q, yb = ya + 1, nx = a.nx, ny = a.ny;
@@ -44,7 +43,7 @@ __device__ __forceinline__ void xf_body(const DemagArgs<T> &a, int bx, int z, in
     const T msT = a.unit_source ? T(1) : (T)a.ms;
     auto in = [&](int j) -> C {
         C v = mk<T>(0, 0);
-        if (j >= nx) return v;  // zero padding beyond the row (Lx > 2 nx)
+        if (PAD && j >= nx) return v;  // zero padding beyond the row (Lx > 2 nx)
         if (!a.mask && !a.ms_map && !a.vf) {
             if (ya < ny) v.x = mc[rowa + j] * msT;
             if (yb < ny) v.y = mc[rowb + j] * msT;
@@ -93,11 +92,10 @@ template <typename T, int L1, int L2>
 __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, int c, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = line_region<L1, L2>();
-    C *tw = reinterpret_cast<C *>(smem_raw);
-    C *region = tw + L;
+    const C *tw = a.twxT;
+    C *region = reinterpret_cast<C *>(smem_raw);
     const int LP = a.lines_x, RB = 2 * LP, nx = a.nx, ny = a.ny, nkx = a.nkx;
     const int y0 = bx * RB;
-    fill_tw4<L1, L2>(tw, a.twx, 1);
     // Z[k] = A[k] + i B[k] (k <= nx), Z[L-k] = conj(A[k]) + i conj(B[k]); DC and
     // Nyquist taken as real.  Row pairs (A, B) sit in adjacent lanes.
     const C *s1row = a.s1 + ((long long)c * a.nz + z) * nkx * ny;
@@ -173,21 +171,19 @@ __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
 // ---------------------------------------------------------------------------
 // y forward (3-D): S1 -> S2, line g = (c, z, kx); block = lines_y groups of L2
 // ---------------------------------------------------------------------------
-template <typename T, int L1, int L2>
+template <typename T, int L1, int L2, bool PAD = false>
 __device__ __forceinline__ void yf_body(const DemagArgs<T> &a, int bx, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = tile_elems(L1, L2);
-    C *tw = reinterpret_cast<C *>(smem_raw);
-    C *region = tw + L;
-    fill_tw4<L1, L2>(tw, a.twy, 1);
-    __syncthreads();
+    const C *tw = a.twyT;
+    C *region = reinterpret_cast<C *>(smem_raw);
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2, ny = a.ny;
     const long long total = 3LL * a.nz * a.nkx;
     const long long g = (long long)bx * a.lines_y + q;
     const bool valid = g < total;
     const C *src = a.s1 + g * ny;
     C *dst = a.s2 + g * L;
-    auto in = [&](int j) -> C { return (valid && j < ny) ? src[j] : mk<T>(0, 0); };
+    auto in = [&](int j) -> C { return (valid && (!PAD || j < ny)) ? src[j] : mk<T>(0, 0); };
     auto out = [&](int k, C v) { if (valid) dst[k] = v; };
     fft4step<L1, L2, false, false, false, true>(t, tw, region + q * TE, in, out);
 }
@@ -203,10 +199,8 @@ template <typename T, int L1, int L2>
 __device__ __forceinline__ void yi_body(const DemagArgs<T> &a, int bx, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = tile_elems(L1, L2);
-    C *tw = reinterpret_cast<C *>(smem_raw);
-    C *region = tw + L;
-    fill_tw4<L1, L2>(tw, a.twy, 1);
-    __syncthreads();
+    const C *tw = a.twyT;
+    C *region = reinterpret_cast<C *>(smem_raw);
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2, ny = a.ny;
     const long long total = 3LL * a.nz * a.nkx;
     const long long g = (long long)bx * a.lines_y + q;
@@ -234,10 +228,11 @@ __global__ void __launch_bounds__(256) k_yi_r(DemagArgs<T> a) {
 // so each thread of the pair holds 3 x nz values and the two halves are summed
 // with one shuffle exchange.
 // ---------------------------------------------------------------------------
-// One column task tid (tid / P = column, tid % P = kz parity); the task index
-// of a warp's lanes must be contiguous and start at a multiple of 32.
+// One column task tid (tid / P = column, h = tid % P = kz parity, passed in by
+// the caller: it is the lane parity, invariant over the caller's loop); the task
+// index of a warp's lanes must be contiguous and start at a multiple of 32.
 template <typename T, int LZ, int P>
-__device__ __forceinline__ void zc_task(const DemagArgs<T> &a, int tid) {
+__device__ __forceinline__ void zc_task(const DemagArgs<T> &a, int tid, int h) {
     using C = cx<T>;
     constexpr int NZL = LZ / P;  // points per thread
     static_assert(P == 1 || P == 2, "z split");
@@ -246,7 +241,6 @@ __device__ __forceinline__ void zc_task(const DemagArgs<T> &a, int tid) {
     const int nz = a.nz, Ly = a.Ly, nkx = a.nkx;
     const long long cs = (long long)nz * nkx * Ly;  // component stride in S2
     const long long zs = (long long)nkx * Ly;
-    const int h = (P == 2) ? (tid & 1) : 0;
     {
         const int col = tid / P;
         const bool valid = col < cols;
@@ -322,8 +316,9 @@ __device__ __forceinline__ void zc_task(const DemagArgs<T> &a, int tid) {
 template <typename T, int LZ, int P>
 __global__ void __launch_bounds__(128) k_zc_r(DemagArgs<T> a) {
     const int span = ((a.nkx * a.Ly * P + 127) / 128) * 128;  // whole pairs and warps iterate together
+    const int h = (P == 2) ? (threadIdx.x & 1) : 0;
     for (int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < span; tid += gridDim.x * blockDim.x)
-        zc_task<T, LZ, P>(a, tid);
+        zc_task<T, LZ, P>(a, tid, h);
 }
 
 // ---------------------------------------------------------------------------
@@ -335,10 +330,8 @@ __global__ void __launch_bounds__(256) k_yc_r(DemagArgs<T> a) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = line_region<L1, L2>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *tw = reinterpret_cast<C *>(smem_raw);
-    C *region = tw + L;
-    fill_tw4<L1, L2>(tw, a.twy, 1);
-    __syncthreads();
+    const C *tw = a.twyT;
+    C *region = reinterpret_cast<C *>(smem_raw);
     const int KB = a.kb_y, ny = a.ny, nkx = a.nkx;
     const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;
     const int comp = q / KB, kxl = q - comp * KB;

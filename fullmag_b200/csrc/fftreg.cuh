@@ -17,6 +17,9 @@
 // consecutive k1) are coalesced.
 #pragma once
 
+#include <cmath>
+#include <vector>
+
 #include "common.cuh"
 
 namespace fm {
@@ -111,6 +114,20 @@ __device__ __forceinline__ void fill_tw4(C *twT, const C *__restrict__ g, int st
         const int k1 = idx / L2, t = idx - k1 * L2;
         twT[idx] = g[stride * k1 * t];
     }
+}
+
+// Host: the same table for a power-of-two length L split as l2_for(L), each
+// entry computed exactly like the plain table exp(-2 pi i k / L) at k = k1 t.
+template <typename T>
+inline std::vector<cx<T>> host_tw4(int L) {
+    const int L2 = l2_for(L);
+    std::vector<cx<T>> t(L);
+    for (int idx = 0; idx < L; ++idx) {
+        const int k = (idx / L2) * (idx % L2);
+        const double a = 2.0 * kPi * (double)k / (double)L;
+        t[idx] = mk<T>((T)std::cos(a), (T)(-std::sin(a)));
+    }
+    return t;
 }
 
 // One line, L2 threads; t = thread index within the line group.

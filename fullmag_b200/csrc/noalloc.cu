@@ -86,12 +86,15 @@ bool setup_device(int dev, unsigned char **out, char *err, uint64_t errlen) {
     return true;
 }
 
-// tw[k] = exp(-2 pi i k / L), computed on the device (no host staging copy).
-__global__ void k_fill_twiddles(double2 *tw, int L) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L; k += gridDim.x * blockDim.x) {
+// tw[k] = exp(-2 pi i k / L), computed on the device (no host staging copy);
+// with L2 > 0 the 4-step table of fftreg.cuh (entry k1 L2 + t holds the value
+// of k = k1 t).
+__global__ void k_fill_twiddles(double2 *tw, int L, int L2) {
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < L; idx += gridDim.x * blockDim.x) {
+        const int k = L2 > 0 ? (idx / L2) * (idx % L2) : idx;
         double sn, cs;
         sincospi(2.0 * (double)k / (double)L, &sn, &cs);
-        tw[k] = make_double2(cs, -sn);
+        tw[idx] = make_double2(cs, -sn);
     }
 }
 
@@ -138,9 +141,9 @@ extern "C" int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uin
         return FULLMAG_FDM_ERR_INVALID;
     }
     const int nkx = (int)nx + 1;
-    // scratch layout (complex elements): twx | twy | twz | S1 | S2
+    // scratch layout (complex elements): twx | twy | twz | twxT | twyT | S1 | S2
     const size_t s1 = (size_t)3 * nz * nkx * ny, s2 = thin ? 0 : (size_t)3 * nz * nkx * Ly;
-    const size_t elems = (size_t)Lx + Ly + Lz + s1 + s2 + 16;
+    const size_t elems = (size_t)2 * Lx + 2 * Ly + Lz + s1 + s2 + 16;
     const size_t need = elems * sizeof(C);
     if (need > kNoAllocScratchBytes) {
         char msg[256];
@@ -162,11 +165,14 @@ extern "C" int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uin
 
     C *p = reinterpret_cast<C *>(base);
     C *twx = p, *twy = twx + Lx, *twz = twy + Ly;
-    C *ps1 = twz + Lz;
+    C *twxT = twz + Lz, *twyT = twxT + Lx;
+    C *ps1 = twyT + Ly;
     C *ps2 = ps1 + s1;
-    k_fill_twiddles<<<(Lx + 255) / 256, 256, 0, st>>>(twx, Lx);
-    k_fill_twiddles<<<(Ly + 255) / 256, 256, 0, st>>>(twy, Ly);
-    k_fill_twiddles<<<(Lz + 255) / 256, 256, 0, st>>>(twz, Lz);
+    k_fill_twiddles<<<(Lx + 255) / 256, 256, 0, st>>>(twx, Lx, 0);
+    k_fill_twiddles<<<(Ly + 255) / 256, 256, 0, st>>>(twy, Ly, 0);
+    k_fill_twiddles<<<(Lz + 255) / 256, 256, 0, st>>>(twz, Lz, 0);
+    k_fill_twiddles<<<(Lx + 255) / 256, 256, 0, st>>>(twxT, Lx, l2_for(Lx));
+    k_fill_twiddles<<<(Ly + 255) / 256, 256, 0, st>>>(twyT, Ly, l2_for(Ly));
 
     DemagArgs<double> a{};
     a.nx = nx; a.ny = ny; a.nz = nz;
@@ -175,6 +181,7 @@ extern "C" int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uin
     a.KZ = thin ? 1 : (int)nz + 1;
     a.KY = (int)ny + 1;
     a.twx = twx; a.twy = twy; a.twz = twz;
+    a.twxT = twxT; a.twyT = twyT;
     a.s1 = ps1; a.s2 = thin ? nullptr : ps2;
     a.spec = octant;
     a.m = m;
@@ -194,10 +201,10 @@ extern "C" int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uin
         constexpr int TE = line_region<L1, L2>();
         const int unit = L2 >= 32 ? 1 : 32 / L2;
         int lp = std::max(unit, (128 / L2) / unit * unit);
-        while (lp > unit && (size_t)(L1 * L2 + lp * TE) * sz > 200 * 1024) lp -= unit;
+        while (lp > unit && (size_t)(lp * TE) * sz > 200 * 1024) lp -= unit;
         a.lines_x = lp;
         thr_x = lp * L2;
-        smx = (size_t)(L1 * L2 + lp * TE) * sz;
+        smx = (size_t)(lp * TE) * sz;
         ok &= cudaFuncSetAttribute(k_xf_r<double, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx) == cudaSuccess;
         ok &= cudaFuncSetAttribute(k_xi_r<double, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx) == cudaSuccess;
     });
@@ -209,17 +216,17 @@ extern "C" int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uin
             constexpr int TE = line_region<L1, L2>();
             const int unit = L2 >= 32 ? 1 : 32 / L2;
             int kb = std::max(unit, (192 / (3 * L2)) / unit * unit);
-            while (kb > unit && (size_t)(L1 * L2 + 3 * kb * TE) * sz > 200 * 1024) kb -= unit;
+            while (kb > unit && (size_t)(3 * kb * TE) * sz > 200 * 1024) kb -= unit;
             a.kb_y = kb;
             thr_y = 3 * kb * L2;
-            smy = (size_t)(L1 * L2 + 3 * kb * TE) * sz;
+            smy = (size_t)(3 * kb * TE) * sz;
             ok &= cudaFuncSetAttribute(k_yc_r<double, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy) == cudaSuccess;
         } else {
             constexpr int TE = tile_elems(L1, L2);
             const int lpb = std::max(1, 128 / L2);
             a.lines_y = lpb;
             thr_y = lpb * L2;
-            smy = (size_t)(L1 * L2 + lpb * TE) * sz;
+            smy = (size_t)(lpb * TE) * sz;
             ok &= cudaFuncSetAttribute(k_yf_r<double, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy) == cudaSuccess;
             ok &= cudaFuncSetAttribute(k_yi_r<double, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy) == cudaSuccess;
         }

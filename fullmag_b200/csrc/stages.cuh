@@ -82,6 +82,10 @@ struct StageArgs {
     double ew[6];
     int nke;
     double dt;
+    // MODE_EVAL: also the next Heun predictor normalize(m + k dt) with the stored
+    // k, the arithmetic of k_combine form 0 (null: not written)
+    T *pred_out;
+    double pred_dt;
 };
 
 __device__ __forceinline__ double warp_reduce(double v, bool is_max) {
@@ -97,6 +101,27 @@ template <typename T>
 __device__ __forceinline__ bool st_active(const StageArgs<T> &a, long long i, double &ms_i) {
     ms_i = a.ms_map ? a.ms_map[i] : a.ms;
     return (!a.mask || a.mask[i] != 0) && (ms_i > 0.0);
+}
+
+// The next Heun predictor of cell i from the state c (its stored values) and
+// k (as stored in T): normalize(m + k dt), the arithmetic of k_combine form 0.
+template <typename T>
+__device__ __forceinline__ void store_predictor(const StageArgs<T> &a, size_t i, size_t n, const double (&c)[3],
+                                                double r0, double r1, double r2) {
+    const double v0 = c[0] + (double)(T)r0 * a.pred_dt;
+    const double v1 = c[1] + (double)(T)r1 * a.pred_dt;
+    const double v2 = c[2] + (double)(T)r2 * a.pred_dt;
+    const double n2 = v0 * v0 + v1 * v1 + v2 * v2;
+    double inv;
+    if (sizeof(T) == 8) {
+        const double nn = sqrt(n2);
+        inv = nn > 0.0 ? 1.0 / nn : 0.0;
+    } else {
+        inv = n2 > 0.0 ? rsqrt(n2) : 0.0;
+    }
+    a.pred_out[i] = (T)(v0 * inv);
+    a.pred_out[n + i] = (T)(v1 * inv);
+    a.pred_out[2 * n + i] = (T)(v2 * inv);
 }
 
 // Exchange field of the boundary tiers at an active cell i = (x, y, z) with
@@ -255,6 +280,10 @@ __global__ void __launch_bounds__(256, 3) k_stage(StageArgs<T> a) {
             if (a.hex_out) { a.hex_out[i] = T(0); a.hex_out[n + i] = T(0); a.hex_out[2 * n + i] = T(0); }
             if (a.heff_out) { a.heff_out[i] = T(0); a.heff_out[n + i] = T(0); a.heff_out[2 * n + i] = T(0); }
             if (MODE == MODE_HEUN_CORR) { a.m0[i] = T(0); a.m0[n + i] = T(0); a.m0[2 * n + i] = T(0); }
+            if (MODE == MODE_EVAL && a.pred_out) {
+                const double c0[3] = {(double)mx[i], (double)my[i], (double)mz[i]};
+                store_predictor(a, (size_t)i, (size_t)n, c0, 0.0, 0.0, 0.0);
+            }
         } else {
             // neighbours: clamped at the grid edge, inactive -> centre (lib.rs:2255-2286)
             long long nb[6];
@@ -323,6 +352,7 @@ __global__ void __launch_bounds__(256, 3) k_stage(StageArgs<T> a) {
             const R r0 = (pr * p0 + q0 * al) * gb, r1 = (pr * p1 + q1 * al) * gb,
                     r2 = (pr * p2 + q2 * al) * gb;
             if (a.kout) { a.kout[i] = (T)r0; a.kout[n + i] = (T)r1; a.kout[2 * n + i] = (T)r2; }
+            if (MODE == MODE_EVAL && a.pred_out) store_predictor(a, (size_t)i, (size_t)n, c3, r0, r1, r2);
             if (a.hex_out) { a.hex_out[i] = (T)h0; a.hex_out[n + i] = (T)h1; a.hex_out[2 * n + i] = (T)h2; }
             if (a.heff_out) { a.heff_out[i] = (T)e0; a.heff_out[n + i] = (T)e1; a.heff_out[2 * n + i] = (T)e2; }
             if (MODE == MODE_HEUN_CORR) {
@@ -496,6 +526,7 @@ __device__ __forceinline__ void stage_plain_body(const StageArgs<T> &a, int zb, 
         const R r0 = (pr * p0 + q0 * al) * gb, r1 = (pr * p1 + q1 * al) * gb, r2 = (pr * p2 + q2 * al) * gb;
         if (inxy) {
             if (a.kout) { a.kout[i] = (T)r0; a.kout[n + i] = (T)r1; a.kout[2 * (size_t)n + i] = (T)r2; }
+            if (MODE == MODE_EVAL && a.pred_out) store_predictor(a, (size_t)i, (size_t)n, c, r0, r1, r2);
             if (a.hex_out) { a.hex_out[i] = (T)h[0]; a.hex_out[n + i] = (T)h[1]; a.hex_out[2 * (size_t)n + i] = (T)h[2]; }
             if (a.heff_out) { a.heff_out[i] = (T)e0; a.heff_out[n + i] = (T)e1; a.heff_out[2 * (size_t)n + i] = (T)e2; }
             if (MODE == MODE_HEUN_CORR) {

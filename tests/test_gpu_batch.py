@@ -64,3 +64,18 @@ def test_batch_reports_errors():
     with nf.NativeFdmBatch(_problems()[:2]) as b:
         with pytest.raises(nf.RunError, match="problem index out of range"):
             b._check(b._lib.fullmag_fdm_batch_copy_m(b._h, 5, np.zeros(3).ctypes.data_as(nf._dp), 3), "copy")
+
+
+def test_batch_dt_change_matches_oracle():
+    probs = _problems()[:3]
+    with nf.NativeFdmBatch(probs, nf.PRECISION_DOUBLE) as b:
+        b.step_n(5e-14, 3)
+        b.step_n(3e-14, 4)
+        for i, p in enumerate(probs):
+            nx, ny, nz = p["cells"]
+            prob = O.Problem(nx, ny, nz, *p["cell_size"], ms=p["ms"], aex=p["aex"], alpha=p["alpha"],
+                             gamma=p["gamma"], h_ext=p["h_ext"])
+            sim = O.Simulation(prob, p["m0"])
+            for dt in [5e-14] * 3 + [3e-14] * 4:
+                sim.step(dt)
+            assert np.abs(b.copy_m(i) - sim.m).max() <= 1e-10, i

@@ -391,3 +391,22 @@ def test_fused_yz_cluster_pass_matches_oracle(monkeypatch, cells, prec):
     tol = 1e-13 if prec == nf.PRECISION_DOUBLE else 2e-6
     for k, v in err.items():
         assert v <= tol, (k, v)
+
+
+def test_heun_dt_change_and_upload_recompute_the_predictor():
+    """The RHS kernel that ends a Heun step also writes the next predictor for
+    the same dt; a different dt, an upload or another integrator's step must
+    not reuse it."""
+    kw = dict(cells=(24, 16, 2), cell_size=(2e-9, 2e-9, 2e-9), alpha=0.1, h_ext=(1e4, 2e4, 0))
+    be, sim, m0 = make_pair(**kw)
+    for dt in [3e-14, 3e-14, 5e-14, 5e-14, 2e-14]:
+        be.step(dt)
+        sim.step(dt)
+    assert max_abs(be.copy_m(), sim.m) <= 1e-10
+    m_new = O.random_unit_vectors(77, 24 * 16 * 2)
+    be.upload_m(m_new)
+    sim.set_m(m_new)
+    for _ in range(3):
+        be.step(2e-14)
+        sim.step(2e-14)
+    assert max_abs(be.copy_m(), sim.m) <= 1e-10
