@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -65,6 +66,11 @@ static bool with_split(int L, F &&f) {
 }
 
 static bool is_pow2(int L) { return L >= 2 && (L & (L - 1)) == 0; }
+
+static bool env_is(const char *name, const char *value) {
+    const char *v = std::getenv(name);
+    return v && std::strcmp(v, value) == 0;
+}
 
 // ---------------------------------------------------------------------------
 // helpers
@@ -188,6 +194,24 @@ struct Impl {
                 b.rsm_x = (size_t)(lp * TE) * sz;
                 ok &= cuda_ok(b, cudaFuncSetAttribute(k_xf_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_x), "attr xf_r");
                 ok &= cuda_ok(b, cudaFuncSetAttribute(k_xi_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_x), "attr xi_r");
+                // pipelined x forward for a uniform material with 16-byte rows
+                b.use_xpipe = false;
+                if (ok && !b.has_mask && !b.has_ms_map && !b.boundary_tier && (b.nx * sizeof(T)) % 16 == 0) {
+                    const int RB = 2 * lp;
+                    const size_t smem = xpipe_region_bytes<L1, L2, T>(lp) + (size_t)2 * RB * b.nx * sizeof(T);
+                    int occ = 0, sms = 148;
+                    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.device);
+                    if (smem <= 200 * 1024 &&
+                        cudaFuncSetAttribute(k_xf_pipe<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+                        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xf_pipe<T, L1, L2>, b.thr_x, smem) == cudaSuccess &&
+                        occ > 0 && !env_is("FULLMAG_FDM_XPIPE", "off")) {
+                        b.groups_x = 3 * b.nz * ((b.ny + RB - 1) / RB);
+                        b.grid_xpipe = std::min(b.groups_x, occ * sms);
+                        b.rsm_xpipe = smem;
+                        b.use_xpipe = true;
+                    }
+                    cudaGetLastError();
+                }
             }
         });
         if (!ok) return false;
@@ -228,7 +252,10 @@ struct Impl {
             constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
             if constexpr (!(sizeof(T) == 8 && L1 > 32)) {
                 ProfScope p(b, "demag_x_fwd");
-                k_xf_r<T, L1, L2><<<gx, b.thr_x, b.rsm_x, b.stream>>>(a);
+                if (b.use_xpipe)
+                    k_xf_pipe<T, L1, L2><<<b.grid_xpipe, b.thr_x, b.rsm_xpipe, b.stream>>>(a, b.groups_x);
+                else
+                    k_xf_r<T, L1, L2><<<gx, b.thr_x, b.rsm_x, b.stream>>>(a);
             }
         });
         if (b.thin) {

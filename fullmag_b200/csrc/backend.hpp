@@ -93,6 +93,9 @@ struct Backend {
     bool use_reg = false;
     bool force_stockham = false;  // FULLMAG_FDM_FFT=stockham selects the shared-memory FFT
     int thr_x = 0, thr_y = 0, thr_yc = 0;
+    bool use_xpipe = false;       // uniform material: cp.async-pipelined x forward
+    size_t rsm_xpipe = 0;
+    int grid_xpipe = 0, groups_x = 0;
     bool stage_plain = false;     // uniform material: z-marching stage kernel
     int stage_zb = 1;             // z planes per thread of that kernel
     bool use_yz = false;          // fused y-z cluster pass (3-D, register FFT)

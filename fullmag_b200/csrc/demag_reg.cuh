@@ -85,6 +85,96 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------
+// x forward, uniform material (no mask, Ms map or volume fraction; Lx = 2 nx,
+// rows of 16-byte multiples): persistent blocks walk the groups g = (c, z,
+// y-block) of RB = 2 lines_x rows.  The RB rows of a group are one contiguous
+// chunk of m; the next group's chunk is copied into shared memory with 16-byte
+// cp.async while the current group is transformed (double buffer, one commit
+// group per chunk), so the row loads no longer stall the FFT.  The transform
+// and the transposed store are those of xf_body.
+// Shared memory: lines_x line regions (TE complex each), then 2 x RB nx reals.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <int L1, int L2, typename T>
+__host__ __device__ constexpr size_t xpipe_region_bytes(int lines) {
+    return ((size_t)lines * line_region<L1, L2>() * 2 * sizeof(T) + 15) / 16 * 16;
+}
+
+template <typename T, int L1, int L2>
+__global__ void __launch_bounds__(256) k_xf_pipe(DemagArgs<T> a, int ngroups) {
+    using C = cx<T>;
+    constexpr int L = L1 * L2, TE = line_region<L1, L2>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int LP = a.lines_x, RB = 2 * LP, nx = a.nx, ny = a.ny, nz = a.nz, nkx = a.nkx;
+    const int nyb = (ny + RB - 1) / RB;
+    C *region = reinterpret_cast<C *>(smem_raw);
+    T *stage = reinterpret_cast<T *>(smem_raw + xpipe_region_bytes<L1, L2, T>(LP));
+    const size_t stage_elems = (size_t)RB * nx;
+    constexpr int PER = 16 / (int)sizeof(T);  // elements per 16-byte copy
+    auto issue = [&](int g, int buf) {
+        const int yb = g % nyb, cz = g / nyb, z = cz % nz, c = cz / nz;
+        const int y0 = yb * RB, rows = min(RB, ny - y0);
+        const T *src = a.m + (long long)c * a.n + ((long long)z * ny + y0) * nx;
+        T *dst = stage + buf * stage_elems;
+        const int chunks = rows * nx / PER;
+        for (int u = threadIdx.x; u < chunks; u += blockDim.x) cp_async16(dst + u * PER, src + u * PER);
+        cp_async_commit();
+    };
+    const int q = threadIdx.x / L2, t = threadIdx.x - q * L2;
+    C *line = region + q * TE;
+    const T msT = a.unit_source ? T(1) : (T)a.ms;
+    int buf = 0;
+    if (blockIdx.x < ngroups) issue(blockIdx.x, 0);
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const int gn = g + gridDim.x;
+        if (gn < ngroups) issue(gn, buf ^ 1);
+        else cp_async_commit();  // an empty group keeps "all but the newest" meaning this chunk
+        cp_async_wait_all_but_one();
+        __syncthreads();
+        const int yb = g % nyb, cz = g / nyb, z = cz % nz, c = cz / nz;
+        const int y0 = yb * RB, ya = y0 + 2 * q, yb1 = ya + 1;
+        const T *ra = stage + buf * stage_elems + (size_t)(2 * q) * nx, *rb = ra + nx;
+        auto in = [&](int j) -> C {
+            C v = mk<T>(0, 0);
+            if (ya < ny) v.x = ra[j] * msT;
+            if (yb1 < ny) v.y = rb[j] * msT;
+            return v;
+        };
+        auto out = [&](int k, C v) { line[k] = v; };
+        fft4step<L1, L2, false, false, true, true>(t, a.twxT, line, in, out);
+        __syncthreads();
+        C *s1row = a.s1 + ((long long)c * nz + z) * nkx * ny;
+        auto emit = [&](int k, int r) {
+            const int y = y0 + r;
+            if (y >= ny) return;
+            const C *ln = region + (r >> 1) * TE;
+            const C zk = ln[k];
+            const C zm = ln[k == 0 ? 0 : L - k];
+            C o;
+            if ((r & 1) == 0) { o.x = T(0.5) * (zk.x + zm.x); o.y = T(0.5) * (zk.y - zm.y); }
+            else { o.x = T(0.5) * (zk.y + zm.y); o.y = T(-0.5) * (zk.x - zm.x); }
+            s1row[(long long)k * ny + y] = o;
+        };
+        if (blockDim.x % RB == 0) {
+            const int r = threadIdx.x % RB, kstep = blockDim.x / RB;
+            for (int k = threadIdx.x / RB; k < nkx; k += kstep) emit(k, r);
+        } else {
+            for (int u = threadIdx.x; u < nkx * RB; u += blockDim.x) emit(u / RB, u % RB);
+        }
+        __syncthreads();  // the line regions and this buffer are reused
+        buf ^= 1;
+    }
+    // retire the copy groups still in flight (none land in memory still read)
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
 // x inverse: gather A/B half spectra (transposed), form Z = A + iB on the full
 // circle, C2R, crop, 1/P, mask.  Same grid as k_xf_r.
 // ---------------------------------------------------------------------------

@@ -340,7 +340,7 @@ def test_runtime_errors_are_reported():
     assert lib.fullmag_fdm_backend_last_error(be.handle) == b"out_len mismatch"
 
 
-@pytest.mark.parametrize("fft", ["register", "fused", "stockham"])
+@pytest.mark.parametrize("fft", ["register", "fused", "stockham", "xpipe-off"])
 @pytest.mark.parametrize("cells,prec", [((64, 16, 1), nf.PRECISION_DOUBLE), ((32, 16, 8), nf.PRECISION_DOUBLE),
                                         ((32, 16, 8), nf.PRECISION_SINGLE), ((64, 32, 16), nf.PRECISION_SINGLE),
                                         ((256, 64, 1), nf.PRECISION_DOUBLE)])
@@ -357,6 +357,12 @@ def test_both_fft_paths_match_oracle(monkeypatch, fft, cells, prec):
         monkeypatch.setenv("FULLMAG_FDM_YZ", "fused")
     else:
         monkeypatch.delenv("FULLMAG_FDM_YZ", raising=False)
+    # the pipelined x forward serves uniform materials; "xpipe-off" keeps the
+    # one-group-per-block kernel
+    if fft == "xpipe-off":
+        monkeypatch.setenv("FULLMAG_FDM_XPIPE", "off")
+    else:
+        monkeypatch.delenv("FULLMAG_FDM_XPIPE", raising=False)
     be, sim, _ = make_pair(cells, (2e-9, 2e-9, 2e-9), alpha=0.3, h_ext=(1e4, 0, 2e4), precision=prec,
                            symmetric_kernel=True, seed=7)
     err = _field_errors(be, sim.observe())
