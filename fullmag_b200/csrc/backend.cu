@@ -170,13 +170,32 @@ struct Impl {
         return a;
     }
 
-    // Register-FFT path: power-of-two lengths, x/y <= 1024 (FP64) or 4096
-    // (FP32), z <= 16 (FP64) or 32 (FP32) since a thread holds 3 z lines.
+    // direct z convolution for nz = NZ (runtime nz -> template)
+    template <typename F>
+    static void with_nz(int nz, F &&f) {
+        switch (nz) {
+            case 1: f(std::integral_constant<int, 1>{}); break;
+            case 2: f(std::integral_constant<int, 2>{}); break;
+            case 3: f(std::integral_constant<int, 3>{}); break;
+            case 4: f(std::integral_constant<int, 4>{}); break;
+            case 5: f(std::integral_constant<int, 5>{}); break;
+            case 6: f(std::integral_constant<int, 6>{}); break;
+            case 7: f(std::integral_constant<int, 7>{}); break;
+            case 8: f(std::integral_constant<int, 8>{}); break;
+            default: break;
+        }
+    }
+
+    // Register-FFT path: power-of-two x/y lengths <= 1024 (FP64) or 4096 (FP32).
+    // z: direct summation for nz <= 8 (any nz; FULLMAG_FDM_ZCONV=fft keeps the
+    // z FFT), else the register z FFT, Lz a power of two <= 16 (FP64) or 32
+    // (FP32) since a thread holds 3 z lines.
     static bool configure_reg(Backend &b) {
         const bool dbl = sizeof(T) == 8;
         const int maxxy = dbl ? 1024 : 4096, maxz = dbl ? 16 : 32;
         if (!is_pow2(b.Lx) || !is_pow2(b.Ly) || b.Lx > maxxy || b.Ly > maxxy) return false;
-        if (!b.thin && (!is_pow2(b.Lz) || b.Lz > maxz)) return false;
+        b.zdirect = !b.thin && b.nz <= 8 && !b.want_yz && !env_is("FULLMAG_FDM_ZCONV", "fft");
+        if (!b.thin && !b.zdirect && (!is_pow2(b.Lz) || b.Lz > maxz)) return false;
         const size_t sz = sizeof(C), maxs = 200 * 1024;
         const int target = 128;  // x passes: small blocks, several per SM
         bool ok = true;
@@ -241,6 +260,19 @@ struct Impl {
             }
         });
         if (ok && !b.thin && b.want_yz && !yz_configure<T>(b)) return false;
+        if (ok && b.zdirect) {
+            with_nz(b.nz, [&](auto nzc) {
+                constexpr int NZ = decltype(nzc)::value;
+                const size_t smem = (size_t)zd_threads<T>() * zd_smem_per_thread<T, NZ>();
+                int occ = 0, sms = 148;
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.device);
+                ok &= cuda_ok(b, cudaFuncSetAttribute(k_zd<T, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr zd");
+                ok &= cuda_ok(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_zd<T, NZ>, zd_threads<T>(), smem), "occupancy zd");
+                const long long cols = (long long)b.nkx * b.Ly;
+                b.grid_zd = (int)std::max<long long>(1, std::min<long long>((cols + zd_threads<T>() - 1) / zd_threads<T>(), (long long)std::max(occ, 1) * sms));
+                b.rsm_zd = smem;
+            });
+        }
         return ok;
     }
 
@@ -279,7 +311,13 @@ struct Impl {
                     k_yf_r<T, L1, L2><<<gy, b.thr_y, b.rsm_y, b.stream>>>(a);
                 }
             });
-            {
+            if (b.zdirect) {
+                ProfScope p(b, "demag_z_direct");
+                with_nz(b.nz, [&](auto nzc) {
+                    constexpr int NZ = decltype(nzc)::value;
+                    k_zd<T, NZ><<<b.grid_zd, zd_threads<T>(), b.rsm_zd, b.stream>>>(a);
+                });
+            } else {
                 ProfScope p(b, "demag_z_conv");
                 const long long cols = (long long)b.nkx * b.Ly;
                 // one thread per column up to 3 x 8 z points, a thread pair (split by
@@ -320,6 +358,7 @@ struct Impl {
             return true;
         }
         b.use_reg = false;
+        b.zdirect = false;
         if (!b.last_error.empty()) return false;
         const int budget = 100 * 1024;
         const int sz = (int)sizeof(C);
@@ -1117,10 +1156,14 @@ static bool upload_tables(Backend &b, const std::vector<double> (&spec)[6]) {
         return cuda_ok(b, cudaMemcpy(dst, t.data(), L * sizeof(cx<T>), cudaMemcpyHostToDevice), "twiddles (4-step)");
     };
     if (!tw4(b.Lx, b.twxT) || !tw4(b.Ly, b.twyT)) return false;
-    const size_t plane = (size_t)b.KZ * b.nkx * b.KY;
+    // the octant, or for the direct z convolution its z-inverse table (nz planes)
+    std::vector<double> zt[6];
+    if (b.zdirect) octant_to_z_direct(b.nkx, b.KY, b.nz, spec, zt);
+    const auto &src = b.zdirect ? zt : spec;
+    const size_t plane = (size_t)(b.zdirect ? b.nz : b.KZ) * b.nkx * b.KY;
     std::vector<T> host(6 * plane);
     for (int c = 0; c < 6; ++c)
-        for (size_t o = 0; o < plane; ++o) host[c * plane + o] = (T)spec[c][o];
+        for (size_t o = 0; o < plane; ++o) host[c * plane + o] = (T)src[c][o];
     return cuda_ok(b, cudaMemcpy(b.spec, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice), "spectra upload");
 }
 

@@ -353,10 +353,28 @@ __device__ __forceinline__ void zc_task(const DemagArgs<T> &a, int tid, int h) {
         fft_reg<NZL, false>(vy);
         fft_reg<NZL, false>(vz);
         if (valid) {
+            // tensor_apply for one (kx, ky) column: the ky mirror, its sign and the
+            // column's offset in a kz plane of the octant are hoisted out of the kz
+            // loop; 32-bit offsets (6 KZ nkx KY < 2^31 for every supported grid)
+            const int KY = a.KY, plane_z = nkx * KY, cstr = a.KZ * plane_z;
+            const bool ymir = ky > Ly / 2;
+            const T sy = ymir ? T(-1) : T(1);
+            const T *sp = a.spec + (kx * KY + (ymir ? Ly - ky : ky));
 #pragma unroll
             for (int p = 0; p < NZL; ++p) {
                 const int kz = P * brev<NZL>(p) + h;
-                tensor_apply(a, kx, ky, kz, vx[p], vy[p], vz[p]);
+                const bool zmir = kz > LZ / 2;
+                const T sz = zmir ? T(-1) : T(1);
+                const T *q = sp + (zmir ? LZ - kz : kz) * plane_z;
+                const T nxx = q[0], nyy = q[cstr], nzz = q[2 * cstr];
+                const T nxy = q[3 * cstr] * sy, nxz = q[4 * cstr] * sz, nyz = q[5 * cstr] * (sy * sz);
+                const C mx = vx[p], my = vy[p], mz = vz[p];
+                vx[p].x = -((nxx * mx.x + nxy * my.x) + nxz * mz.x);
+                vx[p].y = -((nxx * mx.y + nxy * my.y) + nxz * mz.y);
+                vy[p].x = -((nxy * mx.x + nyy * my.x) + nyz * mz.x);
+                vy[p].y = -((nxy * mx.y + nyy * my.y) + nyz * mz.y);
+                vz[p].x = -((nxz * mx.x + nyz * my.x) + nzz * mz.x);
+                vz[p].y = -((nxz * mx.y + nyz * my.y) + nzz * mz.y);
             }
         }
         fft_reg_dit<NZL, true>(vx);
@@ -410,6 +428,135 @@ __global__ void __launch_bounds__(128) k_zc_r(DemagArgs<T> a) {
     for (int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < span; tid += gridDim.x * blockDim.x)
         zc_task<T, LZ, P>(a, tid, h);
 }
+
+// ---------------------------------------------------------------------------
+// z convolution by direct summation (3-D, nz <= 8).  With the zero padding the
+// FFT pass computes, per (kx, ky) column, the linear convolution
+//   H(z) = -sum_{z' < nz} n(z - z') M(z'),   n(d) = sum_kz N(kx, ky, kz) W_Lz^{-kz d},
+// and only offsets |d| < nz reach a kept output, so the same sum is taken here
+// directly: nz^2 3x3 tensor products per column instead of the two z FFTs,
+// no twiddles and no padded points.  The table (built on the host from the
+// octant, newell_host.hpp octant_to_z_direct) holds n(d) for d in [0, nz):
+// components even in z are real; xz and yz are i tau(d) with tau real and odd
+// in d.  With Mz' = -i Mz and Hz' = -i Hz the product is a real matrix on
+// complex vectors,
+//   (Hx, Hy, Hz') = [[-nxx, -nxy, tau_xz], [-nxy, -nyy, tau_yz],
+//                    [-tau_xz, -tau_yz, -nzz]] (Mx, My, Mz'),
+// stored as tab[c][d][kx][ky'] = (-nxx, -nyy, -nzz, -nxy, tau_xz, tau_yz) for
+// ky' <= Ly/2.  ky > Ly/2 reads the mirror with the sign of the components odd
+// in y (xy, yz); d < 0 flips the components odd in z (xz, yz).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void zd_fma(float2 &h, float c, float2 m) {
+    h = __ffma2_rn(make_float2(c, c), m, h);  // packed: one instruction for both parts
+}
+__device__ __forceinline__ void zd_fma(double2 &h, double c, double2 m) {
+    h.x = fma(c, m.x, h.x);
+    h.y = fma(c, m.y, h.y);
+}
+
+// cp.async of one 4-, 8- or 16-byte element (16: L2 only)
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(unsigned smem, const void *gmem) {
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Persistent threads, one column per thread per iteration; the
+// next column's inputs and table entries are copied into the thread's own
+// shared-memory slots (cp.async, double buffer) while the current one is
+// summed, so the loads of one column overlap the arithmetic of the previous.
+// A thread only reads back what it copied itself: no block barrier.
+// Shared memory per thread: 2 x (3 nz complex + 6 nz reals), item-major with
+// the thread index fastest (conflict-free).
+template <typename T, int NZ>
+__host__ __device__ constexpr size_t zd_smem_per_thread() {
+    return 2 * (3 * NZ * sizeof(cx<T>) + 6 * NZ * sizeof(T));
+}
+template <typename T> __host__ __device__ constexpr int zd_threads() { return sizeof(T) == 8 ? 64 : 128; }
+
+template <typename T, int NZ>
+__global__ void __launch_bounds__(zd_threads<T>()) k_zd(DemagArgs<T> a) {
+    using C = cx<T>;
+    constexpr int NM = 3 * NZ, NT = 6 * NZ, BT = zd_threads<T>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x;
+    C *mb0 = reinterpret_cast<C *>(smem_raw);
+    T *tb0 = reinterpret_cast<T *>(mb0 + 2 * NM * BT);
+    // 3 NZ nkx Ly and 6 NZ nkx KY < 2^31 for every supported grid: 32-bit offsets
+    const int Ly = a.Ly, KY = a.KY, cols = a.nkx * Ly;
+    const int cs = NZ * cols, dstr = a.nkx * KY, tstr = NZ * dstr;
+    auto prefetch = [&](int col, int buf) {
+        const int kx = col / Ly, ky = col - kx * Ly;
+        const C *src = a.s2 + col;
+        const unsigned dm = (unsigned)__cvta_generic_to_shared(mb0 + buf * NM * BT + tid);
+#pragma unroll
+        for (int s = 0; s < NM; ++s)
+            cp_async_elem<sizeof(C)>(dm + s * BT * (unsigned)sizeof(C), src + (s / NZ) * cs + (s % NZ) * cols);
+        const T *tp = a.spec + (kx * KY + (ky > Ly / 2 ? Ly - ky : ky));
+        const unsigned dt = (unsigned)__cvta_generic_to_shared(tb0 + buf * NT * BT + tid);
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+#pragma unroll
+            for (int d = 0; d < NZ; ++d)
+                if (c < 4 || d > 0)  // tau(0) = 0 is not read
+                    cp_async_elem<sizeof(T)>(dt + (c * NZ + d) * BT * (unsigned)sizeof(T), tp + c * tstr + d * dstr);
+    };
+    const int stride = gridDim.x * BT;
+    int col = blockIdx.x * BT + tid, buf = 0;
+    if (col < cols) prefetch(col, 0);
+    cp_async_commit();
+    for (; col < cols; col += stride, buf ^= 1) {
+        if (col + stride < cols) prefetch(col + stride, buf ^ 1);
+        cp_async_commit();  // possibly empty: "all but the newest" is this column
+        cp_async_wait_all_but_one();
+        const C *sm = mb0 + buf * NM * BT + tid;
+        const T *st = tb0 + buf * NT * BT + tid;
+        const int kx = col / Ly, ky = col - kx * Ly;
+        const T sy = ky > Ly / 2 ? T(-1) : T(1);
+        C mx[NZ], my[NZ], mz[NZ], hx[NZ], hy[NZ], hz[NZ];
+#pragma unroll
+        for (int z = 0; z < NZ; ++z) {
+            mx[z] = sm[z * BT];
+            my[z] = sm[(NZ + z) * BT];
+            const C v = sm[(2 * NZ + z) * BT];
+            mz[z] = mk<T>(v.y, -v.x);  // -i Mz
+            hx[z] = mk<T>(0, 0); hy[z] = mk<T>(0, 0); hz[z] = mk<T>(0, 0);
+        }
+#pragma unroll
+        for (int d = 0; d < NZ; ++d) {
+            const T cxx = st[d * BT], cyy = st[(NZ + d) * BT], czz = st[(2 * NZ + d) * BT];
+            const T cxy = st[(3 * NZ + d) * BT] * sy;
+            const T cxz = d > 0 ? st[(4 * NZ + d) * BT] : T(0), cyz = d > 0 ? st[(5 * NZ + d) * BT] * sy : T(0);
+#pragma unroll
+            for (int z = 0; z + d < NZ; ++z) {
+                {   // output z + d from input z (offset +d)
+                    const int o = z + d;
+                    zd_fma(hx[o], cxx, mx[z]); zd_fma(hx[o], cxy, my[z]); zd_fma(hx[o], cxz, mz[z]);
+                    zd_fma(hy[o], cxy, mx[z]); zd_fma(hy[o], cyy, my[z]); zd_fma(hy[o], cyz, mz[z]);
+                    zd_fma(hz[o], -cxz, mx[z]); zd_fma(hz[o], -cyz, my[z]); zd_fma(hz[o], czz, mz[z]);
+                }
+                if (d > 0) {  // output z from input z + d (offset -d: odd-in-z entries flip)
+                    const int i = z + d;
+                    zd_fma(hx[z], cxx, mx[i]); zd_fma(hx[z], cxy, my[i]); zd_fma(hx[z], -cxz, mz[i]);
+                    zd_fma(hy[z], cxy, mx[i]); zd_fma(hy[z], cyy, my[i]); zd_fma(hy[z], -cyz, mz[i]);
+                    zd_fma(hz[z], cxz, mx[i]); zd_fma(hz[z], cyz, my[i]); zd_fma(hz[z], czz, mz[i]);
+                }
+            }
+        }
+        C *base = a.s2 + col;
+#pragma unroll
+        for (int z = 0; z < NZ; ++z) {
+            base[z * cols] = hx[z];
+            base[cs + z * cols] = hy[z];
+            base[2 * cs + z * cols] = mk<T>(-hz[z].y, hz[z].x);  // Hz = i Hz'
+        }
+    }
+    cp_async_wait_all();
+}
+
 
 // ---------------------------------------------------------------------------
 // y convolution (2-D thin film): block = kb_y kx columns x 3 components, each

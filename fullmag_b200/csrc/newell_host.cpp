@@ -268,4 +268,34 @@ void newell_octant_spectra_padded(int nx, int ny, int nz, double dx, double dy, 
     }
 }
 
+void octant_to_z_direct(int nkx, int KY, int nz, const std::vector<double> (&spec)[6],
+                        std::vector<double> (&out)[6]) {
+    const size_t plane = (size_t)nkx * KY;
+    const bool oddz[6] = {false, false, false, false, true, true};
+    // cos / sin (pi k d / nz) for k, d < nz
+    std::vector<double> cs((size_t)nz * nz), sn((size_t)nz * nz);
+    for (int d = 0; d < nz; ++d)
+        for (int k = 0; k < nz; ++k) {
+            const double a = PI * (double)k * (double)d / (double)nz;
+            cs[d * nz + k] = std::cos(a);
+            sn[d * nz + k] = std::sin(a);
+        }
+    for (int c = 0; c < 6; ++c) {
+        out[c].assign((size_t)nz * plane, 0.0);
+        const double *S = spec[c].data();
+        double *O = out[c].data();
+        const double sign = oddz[c] ? 1.0 : -1.0;
+        parallel_for(plane, [&](size_t o) {
+            for (int d = 0; d < nz; ++d) {
+                double acc = 0.0;
+                for (int k = 1; k < nz; ++k)
+                    acc += S[(size_t)k * plane + o] * (oddz[c] ? sn[d * nz + k] : cs[d * nz + k]);
+                acc *= 2.0;
+                if (!oddz[c]) acc += S[o] + ((d & 1) ? -1.0 : 1.0) * S[(size_t)nz * plane + o];
+                O[(size_t)d * plane + o] = sign * acc;
+            }
+        });
+    }
+}
+
 }  // namespace fm

@@ -340,15 +340,16 @@ def test_runtime_errors_are_reported():
     assert lib.fullmag_fdm_backend_last_error(be.handle) == b"out_len mismatch"
 
 
-@pytest.mark.parametrize("fft", ["register", "fused", "stockham", "xpipe-off"])
+@pytest.mark.parametrize("fft", ["register", "fused", "stockham", "xpipe-off", "zfft"])
 @pytest.mark.parametrize("cells,prec", [((64, 16, 1), nf.PRECISION_DOUBLE), ((32, 16, 8), nf.PRECISION_DOUBLE),
                                         ((32, 16, 8), nf.PRECISION_SINGLE), ((64, 32, 16), nf.PRECISION_SINGLE),
                                         ((256, 64, 1), nf.PRECISION_DOUBLE)])
 def test_both_fft_paths_match_oracle(monkeypatch, fft, cells, prec):
     """The register-FFT kernels (power-of-two lengths; the y-z convolution as
-    three kernels, or fused per kx plane with FULLMAG_FDM_YZ=fused) and the
-    shared-memory Stockham kernels (any 2,3,5,7-smooth length; forced by
-    FULLMAG_FDM_FFT)."""
+    three kernels, or fused per kx plane with FULLMAG_FDM_YZ=fused; the z
+    convolution summed directly for nz <= 8, or by z FFTs with
+    FULLMAG_FDM_ZCONV=fft) and the shared-memory Stockham kernels (any
+    2,3,5,7-smooth length; forced by FULLMAG_FDM_FFT)."""
     if fft == "stockham":
         monkeypatch.setenv("FULLMAG_FDM_FFT", "stockham")
     else:
@@ -363,12 +364,56 @@ def test_both_fft_paths_match_oracle(monkeypatch, fft, cells, prec):
         monkeypatch.setenv("FULLMAG_FDM_XPIPE", "off")
     else:
         monkeypatch.delenv("FULLMAG_FDM_XPIPE", raising=False)
+    if fft == "zfft":
+        monkeypatch.setenv("FULLMAG_FDM_ZCONV", "fft")
+    else:
+        monkeypatch.delenv("FULLMAG_FDM_ZCONV", raising=False)
     be, sim, _ = make_pair(cells, (2e-9, 2e-9, 2e-9), alpha=0.3, h_ext=(1e4, 0, 2e4), precision=prec,
                            symmetric_kernel=True, seed=7)
+    be.set_profiling(True)
+    be.refresh_observables()
+    names = set(be.profile())
+    be.set_profiling(False)
+    if cells[2] > 1:
+        direct = fft in ("register", "xpipe-off") and cells[2] <= 8
+        assert ("demag_z_direct" in names) == direct, (fft, names)
     err = _field_errors(be, sim.observe())
     tol = 1e-13 if prec == nf.PRECISION_DOUBLE else 2e-6
     for k, v in err.items():
         assert v <= tol, (fft, k, v)
+    for _ in range(5):
+        be.step(2e-14)
+        sim.step(2e-14)
+    assert max_abs(be.copy_m(), sim.m) <= (1e-12 if prec == nf.PRECISION_DOUBLE else 1e-6)
+
+
+# Direct z summation for every nz <= 8, also where 2 nz is not a power of two
+# (those grids ran the Stockham FFT before): nz = 3, 5, 6, 7, both precisions,
+# with a mask and an Ms map on one of them (general stage kernel, masked source).
+@pytest.mark.parametrize("cells,prec", [((32, 16, 3), nf.PRECISION_DOUBLE), ((32, 16, 5), nf.PRECISION_SINGLE),
+                                        ((16, 32, 6), nf.PRECISION_DOUBLE), ((16, 8, 7), nf.PRECISION_SINGLE),
+                                        ((64, 32, 7), nf.PRECISION_DOUBLE)])
+def test_direct_z_convolution_any_nz_matches_oracle(monkeypatch, cells, prec):
+    for k in ("FULLMAG_FDM_FFT", "FULLMAG_FDM_YZ", "FULLMAG_FDM_ZCONV", "FULLMAG_FDM_XPIPE"):
+        monkeypatch.delenv(k, raising=False)
+    nx, ny, nz = cells
+    kw = {}
+    if cells == (16, 32, 6):
+        rng = np.random.default_rng(5)
+        mask = (rng.random(nx * ny * nz) > 0.2).astype(np.uint8)
+        kw = dict(mask=mask)
+    be, sim, _ = make_pair(cells, (2e-9, 2.5e-9, 3e-9), alpha=0.3, h_ext=(1e4, -5e3, 2e4), precision=prec,
+                           symmetric_kernel=True, seed=13, **kw)
+    be.set_profiling(True)
+    be.refresh_observables()
+    names = set(be.profile())
+    be.set_profiling(False)
+    assert "demag_z_direct" in names, names
+    err = _field_errors(be, sim.observe())
+    print(cells, prec, {k: f"{v:.2e}" for k, v in err.items()})
+    tol = 1e-13 if prec == nf.PRECISION_DOUBLE else 2e-6
+    for k, v in err.items():
+        assert v <= tol, (k, v)
     for _ in range(5):
         be.step(2e-14)
         sim.step(2e-14)
