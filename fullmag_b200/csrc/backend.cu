@@ -351,6 +351,22 @@ struct Impl {
         return check_launch(b, "demag (register FFT)");
     }
 
+    // the ring-fed stage kernels' shared memory (above 48 KB for FP64)
+    static bool configure_stage(Backend &b) {
+        if (!b.stage_plain) return true;
+        b.stage_ring = !env_is("FULLMAG_FDM_STAGE", "plain");
+        if (!b.stage_ring) return true;
+        const int thr = 32 * kStagePlainBY;
+        bool ok = true;
+        ok &= cuda_ok(b, cudaFuncSetAttribute(k_stage_ring<T, MODE_EVAL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)ring_bytes<T, MODE_EVAL>(thr)), "attr stage ring");
+        ok &= cuda_ok(b, cudaFuncSetAttribute(k_stage_ring<T, MODE_HEUN_CORR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)ring_bytes<T, MODE_HEUN_CORR>(thr)), "attr stage ring");
+        ok &= cuda_ok(b, cudaFuncSetAttribute(k_stage_ring<T, MODE_ERR_LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)ring_bytes<T, MODE_ERR_LAST>(thr)), "attr stage ring");
+        return ok;
+    }
+
     static bool configure(Backend &b) {
         if (!upload_tw64(b)) return false;
         if (!b.force_stockham && configure_reg(b)) {
@@ -499,7 +515,11 @@ struct Impl {
         if (b.stage_plain) {
             const dim3 g((b.nx + 31) / 32, (b.ny + kStagePlainBY - 1) / kStagePlainBY,
                          (b.nz + b.stage_zb - 1) / b.stage_zb);
-            k_stage_plain<T, MODE><<<g, dim3(32, kStagePlainBY, 1), 0, b.stream>>>(s, b.stage_zb);
+            if (b.stage_ring)
+                k_stage_ring<T, MODE><<<g, dim3(32, kStagePlainBY, 1), ring_bytes<T, MODE>(32 * kStagePlainBY),
+                                        b.stream>>>(s, b.stage_zb);
+            else
+                k_stage_plain<T, MODE><<<g, dim3(32, kStagePlainBY, 1), 0, b.stream>>>(s, b.stage_zb);
         } else {
             k_stage<T, MODE><<<stage_grid(b), dim3(32, 4, 2), 0, b.stream>>>(s);
         }
@@ -1174,6 +1194,8 @@ bool backend_upload_tables(Backend &b, const std::vector<double> (&spec)[6]) {
 }
 
 bool backend_configure(Backend &b) {
+    const bool dbl = b.precision == FULLMAG_FDM_PRECISION_DOUBLE;
+    if (!(dbl ? Impl<double>::configure_stage(b) : Impl<float>::configure_stage(b))) return false;
     if (!b.enable_demag) return true;
     return b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::configure(b)
                                                        : Impl<float>::configure(b);

@@ -97,6 +97,7 @@ struct Backend {
     size_t rsm_xpipe = 0;
     int grid_xpipe = 0, groups_x = 0;
     bool stage_plain = false;     // uniform material: z-marching stage kernel
+    bool stage_ring = false;      // ... fed by the cp.async plane ring (FULLMAG_FDM_STAGE=plain: register prefetch)
     int stage_zb = 1;             // z planes per thread of that kernel
     bool use_yz = false;          // fused y-z cluster pass (3-D, register FFT)
     bool want_yz = false;         // FULLMAG_FDM_YZ=fused selects it (default: three y/z kernels)

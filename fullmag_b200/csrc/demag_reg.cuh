@@ -8,6 +8,7 @@
 // register limits; other lengths use demag.cuh.
 #pragma once
 
+#include "cpasync.cuh"
 #include "demag.cuh"
 #include "fftreg.cuh"
 
@@ -94,12 +95,6 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
 // and the transposed store are those of xf_body.
 // Shared memory: lines_x line regions (TE complex each), then 2 x RB nx reals.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <int L1, int L2, typename T>
 __host__ __device__ constexpr size_t xpipe_region_bytes(int lines) {
@@ -453,16 +448,6 @@ __device__ __forceinline__ void zd_fma(double2 &h, double c, double2 m) {
     h.x = fma(c, m.x, h.x);
     h.y = fma(c, m.y, h.y);
 }
-
-// cp.async of one 4-, 8- or 16-byte element (16: L2 only)
-template <int BYTES>
-__device__ __forceinline__ void cp_async_elem(unsigned smem, const void *gmem) {
-    if constexpr (BYTES == 16)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem), "l"(gmem) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem), "l"(gmem), "n"(BYTES) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Persistent threads, one column per thread per iteration; the
 // next column's inputs and table entries are copied into the thread's own

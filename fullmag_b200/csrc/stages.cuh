@@ -18,6 +18,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "cpasync.cuh"
 
 namespace fm {
 
@@ -437,6 +438,121 @@ struct PlaneLoads {
     T hd[3];   // H_d(x, y, z)
 };
 
+// Cell-invariant values of the uniform-material stage kernels.
+struct PlainConst {
+    double ix2, iy2, iz2, pref, hx0, hx1, hx2, al, gb, pr, coef, pair;
+};
+
+template <typename T>
+__device__ __forceinline__ PlainConst plain_const(const StageArgs<T> &a) {
+    PlainConst k;
+    k.ix2 = a.dinv[0]; k.iy2 = a.dinv[1]; k.iz2 = a.dinv[2];
+    k.pref = a.ex_pref;
+    const double sinv = (a.ac_omega != 0.0) ? sin(a.t * a.ac_omega) : 0.0;
+    k.hx0 = a.has_ext ? a.hext[0] + a.hac[0] * sinv : 0.0;
+    k.hx1 = a.has_ext ? a.hext[1] + a.hac[1] * sinv : 0.0;
+    k.hx2 = a.has_ext ? a.hext[2] + a.hac[2] * sinv : 0.0;
+    k.al = a.alpha; k.gb = -a.gamma_bar;
+    k.pr = a.precession ? 1.0 : 0.0;
+    k.coef = a.ms * a.vol * kMu0;
+    k.pair = a.aex * a.vol;
+    return k;
+}
+
+// Per-cell arithmetic of the uniform-material stage kernels, after the loads:
+// cell i at plane z with m = c, m(z - 1) = dn, m(z + 1) = upT (only read when
+// z + 1 < nz), x neighbours xpT / xmT (already the cell itself at the grid
+// edge), y neighbours ypT / ymT (read only when they exist), H_d = hdT, and for
+// the corrector m0v, k1v.  Stores the stage outputs and accumulates the
+// diagnostics when inxy.
+template <typename T, int MODE>
+__device__ __forceinline__ void plain_cell(const StageArgs<T> &a, const PlainConst &k, unsigned i, unsigned n, int z,
+                                           bool inxy, bool has_xp, bool has_yp, bool has_ym, const double (&c)[3],
+                                           const double (&dn)[3], const T (&upT)[3], const T (&xpT)[3],
+                                           const T (&xmT)[3], const T (&ypT)[3], const T (&ymT)[3],
+                                           const T (&hdT)[3], const T (&m0v)[3], const T (&k1v)[3],
+                                           double (&acc)[NQ]) {
+    using R = double;
+    const int nz = a.nz;
+    const bool ex = a.enable_exchange;
+    R up[3] = {(R)upT[0], (R)upT[1], (R)upT[2]};
+    if (z + 1 >= nz) { up[0] = c[0]; up[1] = c[1]; up[2] = c[2]; }
+    R h[3] = {0.0, 0.0, 0.0};
+    R yp[3], xp[3];
+    if (ex) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            xp[q] = (R)xpT[q];
+            yp[q] = has_yp ? (R)ypT[q] : c[q];
+            const R ym = has_ym ? (R)ymT[q] : c[q];
+            const R lap = (xp[q] - 2.0 * c[q] + (R)xmT[q]) * k.ix2 + (yp[q] - 2.0 * c[q] + ym) * k.iy2 +
+                          (up[q] - 2.0 * c[q] + dn[q]) * k.iz2;
+            h[q] = lap * k.pref;
+        }
+    }
+    const R d0 = hdT[0], d1 = hdT[1], d2 = hdT[2];
+    const R e0 = (h[0] + d0) + k.hx0, e1 = (h[1] + d1) + k.hx1, e2 = (h[2] + d2) + k.hx2;
+    const R cx_ = c[0], cy_ = c[1], cz_ = c[2];
+    const R p0 = cy_ * e2 - cz_ * e1, p1 = cz_ * e0 - cx_ * e2, p2 = cx_ * e1 - cy_ * e0;
+    const R q0 = cy_ * p2 - cz_ * p1, q1 = cz_ * p0 - cx_ * p2, q2 = cx_ * p1 - cy_ * p0;
+    const R r0 = (k.pr * p0 + q0 * k.al) * k.gb, r1 = (k.pr * p1 + q1 * k.al) * k.gb,
+            r2 = (k.pr * p2 + q2 * k.al) * k.gb;
+    if (!inxy) return;
+    if (a.kout) { a.kout[i] = (T)r0; a.kout[n + i] = (T)r1; a.kout[2 * (size_t)n + i] = (T)r2; }
+    if (MODE == MODE_EVAL && a.pred_out) store_predictor(a, (size_t)i, (size_t)n, c, r0, r1, r2);
+    if (a.hex_out) { a.hex_out[i] = (T)h[0]; a.hex_out[n + i] = (T)h[1]; a.hex_out[2 * (size_t)n + i] = (T)h[2]; }
+    if (a.heff_out) { a.heff_out[i] = (T)e0; a.heff_out[n + i] = (T)e1; a.heff_out[2 * (size_t)n + i] = (T)e2; }
+    if (MODE == MODE_HEUN_CORR) {
+        const double hd_ = a.half_dt;
+        const double v0 = (double)m0v[0] + ((double)k1v[0] + r0) * hd_;
+        const double v1 = (double)m0v[1] + ((double)k1v[1] + r1) * hd_;
+        const double v2 = (double)m0v[2] + ((double)k1v[2] + r2) * hd_;
+        const double n2 = v0 * v0 + v1 * v1 + v2 * v2;
+        double inv;
+        if (sizeof(T) == 8) {
+            const double nn = sqrt(n2);
+            inv = nn > 0.0 ? 1.0 / nn : 0.0;
+        } else {
+            inv = n2 > 0.0 ? rsqrt(n2) : 0.0;
+        }
+        a.m0[i] = (T)(v0 * inv); a.m0[n + i] = (T)(v1 * inv); a.m0[2 * (size_t)n + i] = (T)(v2 * inv);
+    }
+    if (a.partials) {
+        if (MODE == MODE_ERR_LAST) {
+            const double rr[3] = {(double)(T)r0, (double)(T)r1, (double)(T)r2};
+            double er[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                double e = 0.0;
+                for (int st = 0; st < a.nke; ++st) e += a.ew[st] * (double)a.ke[st][q * (size_t)n + i];
+                e += a.ew[a.nke] * rr[q];
+                er[q] = e * a.dt;
+            }
+            acc[Q_ERR2] = fmax(acc[Q_ERR2], er[0] * er[0] + er[1] * er[1] + er[2] * er[2]);
+        }
+        if (ex) {
+            // forward pairs (x+1, y+1, z+1) inside the grid, from the loaded neighbours
+            if (has_xp) {
+                const double ddx = xp[0] - cx_, ddy = xp[1] - cy_, ddz = xp[2] - cz_;
+                acc[Q_EEX] += k.pair * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[0];
+            }
+            if (has_yp) {
+                const double ddx = yp[0] - cx_, ddy = yp[1] - cy_, ddz = yp[2] - cz_;
+                acc[Q_EEX] += k.pair * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[1];
+            }
+            if (z + 1 < nz) {
+                const double ddx = up[0] - cx_, ddy = up[1] - cy_, ddz = up[2] - cz_;
+                acc[Q_EEX] += k.pair * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[2];
+            }
+        }
+        acc[Q_EDEMAG] += -0.5 * k.coef * (cx_ * d0 + cy_ * d1 + cz_ * d2);
+        acc[Q_EEXT] += -k.coef * (cx_ * k.hx0 + cy_ * k.hx1 + cz_ * k.hx2);
+        acc[Q_HEFF2] = fmax(acc[Q_HEFF2], e0 * e0 + e1 * e1 + e2 * e2);
+        acc[Q_HD2] = fmax(acc[Q_HD2], d0 * d0 + d1 * d1 + d2 * d2);
+        acc[Q_RHS2] = fmax(acc[Q_RHS2], r0 * r0 + r1 * r1 + r2 * r2);
+    }
+}
+
 // Block body (bx, by, bz); the diagnostics accumulate into acc.  Also run per
 // work item by the batched kernels (batch.cuh).
 template <typename T, int MODE>
@@ -463,17 +579,7 @@ __device__ __forceinline__ void stage_plain_body(const StageArgs<T> &a, int zb, 
         if (dm) { L.hd[0] = a.hd[j]; L.hd[1] = a.hd[n + j]; L.hd[2] = a.hd[2 * (size_t)n + j]; }
         else { L.hd[0] = T(0); L.hd[1] = T(0); L.hd[2] = T(0); }
     };
-    // cell-invariant values
-    const R ix2 = a.dinv[0], iy2 = a.dinv[1], iz2 = a.dinv[2];
-    const R pref = a.ex_pref;
-    const double sinv = (a.ac_omega != 0.0) ? sin(a.t * a.ac_omega) : 0.0;
-    const R hx0 = a.has_ext ? a.hext[0] + a.hac[0] * sinv : 0.0;
-    const R hx1 = a.has_ext ? a.hext[1] + a.hac[1] * sinv : 0.0;
-    const R hx2 = a.has_ext ? a.hext[2] + a.hac[2] * sinv : 0.0;
-    const R al = a.alpha, gb = -a.gamma_bar;
-    const R pr = a.precession ? 1.0 : 0.0;
-    const double coef = a.ms * a.vol * kMu0;
-    const double pair = a.aex * a.vol;
+    const PlainConst k = plain_const(a);
 
     unsigned i = ((unsigned)z0 * (unsigned)ny + (unsigned)yc) * (unsigned)nx + (unsigned)xc;
     T cT[3];
@@ -487,7 +593,7 @@ __device__ __forceinline__ void stage_plain_body(const StageArgs<T> &a, int zb, 
         PlaneLoads<T> Ln;
         if (z + 1 < z1) load_plane(z + 1, i + sxy, Ln);
         // the corrector's m0 and k1 of this cell, issued before the arithmetic
-        T m0v[3], k1v[3];
+        T m0v[3] = {T(0), T(0), T(0)}, k1v[3] = {T(0), T(0), T(0)};
         if (MODE == MODE_HEUN_CORR && inxy) {
             m0v[0] = a.m0[i]; m0v[1] = a.m0[n + i]; m0v[2] = a.m0[2 * (size_t)n + i];
             k1v[0] = a.k1[i]; k1v[1] = a.k1[n + i]; k1v[2] = a.k1[2 * (size_t)n + i];
@@ -495,99 +601,144 @@ __device__ __forceinline__ void stage_plain_body(const StageArgs<T> &a, int zb, 
         // x neighbours: adjacent lanes; the warp's edge lanes load theirs
         T xpT[3], xmT[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            xpT[k] = __shfl_down_sync(0xffffffffu, cT[k], 1);
-            xmT[k] = __shfl_up_sync(0xffffffffu, cT[k], 1);
+        for (int q = 0; q < 3; ++q) {
+            xpT[q] = __shfl_down_sync(0xffffffffu, cT[q], 1);
+            xmT[q] = __shfl_up_sync(0xffffffffu, cT[q], 1);
         }
         if (!has_xp) { xpT[0] = cT[0]; xpT[1] = cT[1]; xpT[2] = cT[2]; }
         else if (lane == 31) ld3(i + 1, xpT);
         if (!has_xm) { xmT[0] = cT[0]; xmT[1] = cT[1]; xmT[2] = cT[2]; }
         else if (lane == 0) ld3(i - 1, xmT);
-        R up[3] = {(R)L.up[0], (R)L.up[1], (R)L.up[2]};
-        if (z + 1 >= nz) { up[0] = c[0]; up[1] = c[1]; up[2] = c[2]; }
-        R h[3] = {0.0, 0.0, 0.0};
-        R yp[3], xp[3];
-        if (ex) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                xp[k] = (R)xpT[k];
-                yp[k] = has_yp ? (R)L.yp[k] : c[k];
-                const R ym = has_ym ? (R)L.ym[k] : c[k];
-                const R lap = (xp[k] - 2.0 * c[k] + (R)xmT[k]) * ix2 + (yp[k] - 2.0 * c[k] + ym) * iy2 +
-                              (up[k] - 2.0 * c[k] + dn[k]) * iz2;
-                h[k] = lap * pref;
-            }
-        }
-        const R d0 = L.hd[0], d1 = L.hd[1], d2 = L.hd[2];
-        const R e0 = (h[0] + d0) + hx0, e1 = (h[1] + d1) + hx1, e2 = (h[2] + d2) + hx2;
-        const R cx_ = c[0], cy_ = c[1], cz_ = c[2];
-        const R p0 = cy_ * e2 - cz_ * e1, p1 = cz_ * e0 - cx_ * e2, p2 = cx_ * e1 - cy_ * e0;
-        const R q0 = cy_ * p2 - cz_ * p1, q1 = cz_ * p0 - cx_ * p2, q2 = cx_ * p1 - cy_ * p0;
-        const R r0 = (pr * p0 + q0 * al) * gb, r1 = (pr * p1 + q1 * al) * gb, r2 = (pr * p2 + q2 * al) * gb;
-        if (inxy) {
-            if (a.kout) { a.kout[i] = (T)r0; a.kout[n + i] = (T)r1; a.kout[2 * (size_t)n + i] = (T)r2; }
-            if (MODE == MODE_EVAL && a.pred_out) store_predictor(a, (size_t)i, (size_t)n, c, r0, r1, r2);
-            if (a.hex_out) { a.hex_out[i] = (T)h[0]; a.hex_out[n + i] = (T)h[1]; a.hex_out[2 * (size_t)n + i] = (T)h[2]; }
-            if (a.heff_out) { a.heff_out[i] = (T)e0; a.heff_out[n + i] = (T)e1; a.heff_out[2 * (size_t)n + i] = (T)e2; }
-            if (MODE == MODE_HEUN_CORR) {
-                const double hd_ = a.half_dt;
-                const double v0 = (double)m0v[0] + ((double)k1v[0] + r0) * hd_;
-                const double v1 = (double)m0v[1] + ((double)k1v[1] + r1) * hd_;
-                const double v2 = (double)m0v[2] + ((double)k1v[2] + r2) * hd_;
-                const double n2 = v0 * v0 + v1 * v1 + v2 * v2;
-                double inv;
-                if (sizeof(T) == 8) {
-                    const double nn = sqrt(n2);
-                    inv = nn > 0.0 ? 1.0 / nn : 0.0;
-                } else {
-                    inv = n2 > 0.0 ? rsqrt(n2) : 0.0;
-                }
-                a.m0[i] = (T)(v0 * inv); a.m0[n + i] = (T)(v1 * inv); a.m0[2 * (size_t)n + i] = (T)(v2 * inv);
-            }
-            if (a.partials) {
-                if (MODE == MODE_ERR_LAST) {
-                    const double rr[3] = {(double)(T)r0, (double)(T)r1, (double)(T)r2};
-                    double er[3];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        double e = 0.0;
-                        for (int st = 0; st < a.nke; ++st) e += a.ew[st] * (double)a.ke[st][k * (size_t)n + i];
-                        e += a.ew[a.nke] * rr[k];
-                        er[k] = e * a.dt;
-                    }
-                    acc[Q_ERR2] = fmax(acc[Q_ERR2], er[0] * er[0] + er[1] * er[1] + er[2] * er[2]);
-                }
-                if (ex) {
-                    // forward pairs (x+1, y+1, z+1) inside the grid, from the loaded neighbours
-                    if (has_xp) {
-                        const double ddx = xp[0] - cx_, ddy = xp[1] - cy_, ddz = xp[2] - cz_;
-                        acc[Q_EEX] += pair * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[0];
-                    }
-                    if (has_yp) {
-                        const double ddx = yp[0] - cx_, ddy = yp[1] - cy_, ddz = yp[2] - cz_;
-                        acc[Q_EEX] += pair * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[1];
-                    }
-                    if (z + 1 < nz) {
-                        const double ddx = up[0] - cx_, ddy = up[1] - cy_, ddz = up[2] - cz_;
-                        acc[Q_EEX] += pair * (ddx * ddx + ddy * ddy + ddz * ddz) * a.dinv[2];
-                    }
-                }
-                acc[Q_EDEMAG] += -0.5 * coef * (cx_ * d0 + cy_ * d1 + cz_ * d2);
-                acc[Q_EEXT] += -coef * (cx_ * hx0 + cy_ * hx1 + cz_ * hx2);
-                acc[Q_HEFF2] = fmax(acc[Q_HEFF2], e0 * e0 + e1 * e1 + e2 * e2);
-                acc[Q_HD2] = fmax(acc[Q_HD2], d0 * d0 + d1 * d1 + d2 * d2);
-                acc[Q_RHS2] = fmax(acc[Q_RHS2], r0 * r0 + r1 * r1 + r2 * r2);
-            }
-        }
+        plain_cell<T, MODE>(a, k, i, n, z, inxy, has_xp, has_yp, has_ym, c, dn, L.up, xpT, xmT, L.yp, L.ym, L.hd,
+                            m0v, k1v, acc);
         // advance one plane
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            dn[k] = c[k];
-            cT[k] = (z + 1 < nz) ? L.up[k] : cT[k];
-            c[k] = (R)cT[k];
+        for (int q = 0; q < 3; ++q) {
+            dn[q] = c[q];
+            cT[q] = (z + 1 < nz) ? L.up[q] : cT[q];
+            c[q] = (R)cT[q];
         }
         L = Ln;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Uniform material, ring-fed: the body of stage_plain_body, but each thread
+// copies the inputs of plane z + D - 1 (m above, the y neighbours, H_d, the
+// warp-edge lane's outer x neighbour, and the corrector's m0 and k1) into its
+// own D-slot shared-memory ring with cp.async while it computes plane z, so
+// D - 1 planes of loads are in flight without holding registers.  A thread
+// reads back only what it copied itself: no block barrier.  Ring layout
+// [slot][item][thread], items of a slot:
+//   0..2 up, 3..5 y+1, 6..8 y-1, 9..11 H_d, 12..14 outer x neighbour (lanes 0
+//   and 31), 15..17 m0 and 18..20 k1 (corrector).
+// ---------------------------------------------------------------------------
+// Depth D and resident blocks per SM, chosen so that D x items x 128 threads of
+// shared memory and the register budget allow that many blocks (measured).
+template <int MODE> __host__ __device__ constexpr int ring_items() { return MODE == MODE_HEUN_CORR ? 21 : 15; }
+template <typename T, int MODE> __host__ __device__ constexpr int ring_depth() {
+    return sizeof(T) == 8 ? 2 : (MODE == MODE_HEUN_CORR ? 3 : 4);
+}
+template <typename T, int MODE> __host__ __device__ constexpr int ring_min_blocks() {
+    return (sizeof(T) == 8 && MODE == MODE_HEUN_CORR) ? 4 : 5;
+}
+template <typename T, int MODE>
+__host__ __device__ constexpr size_t ring_bytes(int threads) {
+    return (size_t)ring_depth<T, MODE>() * ring_items<MODE>() * threads * sizeof(T);
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(128, ring_min_blocks<T, MODE>()) k_stage_ring(StageArgs<T> a, int zb) {
+    using R = double;
+    constexpr int D = ring_depth<T, MODE>(), NV = ring_items<MODE>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *ring = reinterpret_cast<T *>(smem_raw);
+    double acc[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const unsigned n = (unsigned)a.n, sxy = (unsigned)nx * (unsigned)ny;
+    const int lane = threadIdx.x, BT = blockDim.x * blockDim.y, tid = lane + blockDim.x * threadIdx.y;
+    const int x = blockIdx.x * 32 + lane, y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z0 = blockIdx.z * zb, z1 = min(z0 + zb, nz);
+    const bool inxy = x < nx && y < ny;
+    const int xc = min(x, nx - 1), yc = min(y, ny - 1);
+    const T *f0 = a.m, *f1 = a.m + n, *f2 = a.m + 2 * (size_t)n;
+    const bool has_xp = x + 1 < nx, has_xm = x > 0, has_yp = yc + 1 < ny, has_ym = yc > 0;
+    const bool ex = a.enable_exchange, dm = a.enable_demag;
+    const unsigned rbase = (unsigned)__cvta_generic_to_shared(ring + tid);
+    auto item = [&](int z, int v) -> unsigned {  // shared address of item v of plane z's slot
+        return rbase + (unsigned)((((z - z0) % D) * NV + v) * BT) * (unsigned)sizeof(T);
+    };
+    auto cp3 = [&](unsigned dst, const T *p0, const T *p1, const T *p2, unsigned j) {
+        cp_async_elem<sizeof(T)>(dst, p0 + j);
+        cp_async_elem<sizeof(T)>(dst + BT * (unsigned)sizeof(T), p1 + j);
+        cp_async_elem<sizeof(T)>(dst + 2 * BT * (unsigned)sizeof(T), p2 + j);
+    };
+    const unsigned ic = (unsigned)yc * (unsigned)nx + (unsigned)xc;  // in-plane index
+    auto issue = [&](int z) {
+        const unsigned j = (unsigned)z * sxy + ic;
+        if (z + 1 < nz) cp3(item(z, 0), f0, f1, f2, j + sxy);
+        if (ex) {
+            if (has_yp) cp3(item(z, 3), f0, f1, f2, j + nx);
+            if (has_ym) cp3(item(z, 6), f0, f1, f2, j - nx);
+            if (lane == 31 && has_xp) cp3(item(z, 12), f0, f1, f2, j + 1);
+            if (lane == 0 && has_xm) cp3(item(z, 12), f0, f1, f2, j - 1);
+        }
+        if (dm) cp3(item(z, 9), a.hd, a.hd + n, a.hd + 2 * (size_t)n, j);
+        if (MODE == MODE_HEUN_CORR && inxy) {
+            cp3(item(z, 15), a.m0, a.m0 + n, a.m0 + 2 * (size_t)n, j);
+            cp3(item(z, 18), a.k1, a.k1 + n, a.k1 + 2 * (size_t)n, j);
+        }
+    };
+    const PlainConst k = plain_const(a);
+    unsigned i = (unsigned)z0 * sxy + ic;
+    T cT[3] = {f0[i], f1[i], f2[i]};
+    R c[3] = {(R)cT[0], (R)cT[1], (R)cT[2]};
+    R dn[3] = {c[0], c[1], c[2]};
+    if (z0 > 0) { dn[0] = f0[i - sxy]; dn[1] = f1[i - sxy]; dn[2] = f2[i - sxy]; }
+#pragma unroll
+    for (int p = 0; p < D - 1; ++p) {
+        if (z0 + p < z1) issue(z0 + p);
+        cp_async_commit();
+    }
+    for (int z = z0; z < z1; ++z, i += sxy) {
+        if (z + D - 1 < z1) issue(z + D - 1);
+        cp_async_commit();    // possibly empty: the group D - 1 back is always plane z's
+        cp_async_wait<D - 1>();
+        const T *sl = ring + (((z - z0) % D) * NV) * BT + tid;
+        auto rd3 = [&](int v, T (&o)[3]) { o[0] = sl[v * BT]; o[1] = sl[(v + 1) * BT]; o[2] = sl[(v + 2) * BT]; };
+        T upT[3] = {cT[0], cT[1], cT[2]}, ypT[3] = {cT[0], cT[1], cT[2]}, ymT[3] = {cT[0], cT[1], cT[2]};
+        T hdT[3] = {T(0), T(0), T(0)}, m0v[3] = {T(0), T(0), T(0)}, k1v[3] = {T(0), T(0), T(0)};
+        if (z + 1 < nz) rd3(0, upT);
+        if (ex) {
+            if (has_yp) rd3(3, ypT);
+            if (has_ym) rd3(6, ymT);
+        }
+        if (dm) rd3(9, hdT);
+        if (MODE == MODE_HEUN_CORR && inxy) { rd3(15, m0v); rd3(18, k1v); }
+        // x neighbours: adjacent lanes; the warp's edge lanes read their copy
+        T xpT[3], xmT[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            xpT[q] = __shfl_down_sync(0xffffffffu, cT[q], 1);
+            xmT[q] = __shfl_up_sync(0xffffffffu, cT[q], 1);
+        }
+        if (!has_xp) { xpT[0] = cT[0]; xpT[1] = cT[1]; xpT[2] = cT[2]; }
+        else if (lane == 31 && ex) rd3(12, xpT);
+        if (!has_xm) { xmT[0] = cT[0]; xmT[1] = cT[1]; xmT[2] = cT[2]; }
+        else if (lane == 0 && ex) rd3(12, xmT);
+        plain_cell<T, MODE>(a, k, i, n, z, inxy, has_xp, has_yp, has_ym, c, dn, upT, xpT, xmT, ypT, ymT, hdT, m0v,
+                            k1v, acc);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            dn[q] = c[q];
+            cT[q] = (z + 1 < nz) ? upT[q] : cT[q];
+            c[q] = (R)cT[q];
+        }
+    }
+    cp_async_wait_all();
+    if (a.partials) block_reduce_final(acc, a.partials, a.counter, a.out);
 }
 
 template <typename T, int MODE>

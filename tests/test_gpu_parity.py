@@ -461,3 +461,33 @@ def test_heun_dt_change_and_upload_recompute_the_predictor():
         be.step(2e-14)
         sim.step(2e-14)
     assert max_abs(be.copy_m(), sim.m) <= 1e-10
+
+
+# The uniform-material stage kernels come in two forms that share the per-cell
+# arithmetic: loads prefetched one plane ahead into registers
+# (FULLMAG_FDM_STAGE=plain), or copied several planes ahead into a per-thread
+# shared-memory ring (default).  They must agree bit for bit: the state, every
+# field, and every step statistic, also for DP45's last stage (error norm) and
+# on grids whose edges cut warps and blocks.
+@pytest.mark.parametrize("prec", [nf.PRECISION_DOUBLE, nf.PRECISION_SINGLE])
+@pytest.mark.parametrize("integrator", [nf.HEUN, nf.DP45])
+def test_stage_ring_matches_register_prefetch(monkeypatch, prec, integrator):
+    kw = dict(cells=(40, 25, 5), cell_size=(2e-9, 2e-9, 2.5e-9), alpha=0.2, h_ext=(1e4, -2e4, 5e3),
+              precision=prec, integrator=integrator, seed=21)
+    if integrator == nf.DP45:
+        kw["adaptive"] = (1e-6, 1e-16, 1e-12, 0.8)
+    monkeypatch.delenv("FULLMAG_FDM_STAGE", raising=False)
+    ring, _, _ = make_pair(**kw)
+    monkeypatch.setenv("FULLMAG_FDM_STAGE", "plain")
+    plain, _, _ = make_pair(**kw)
+    for k in range(6):
+        dt = 2e-14 if k < 3 else 3e-14
+        sa, sb = ring.step(dt), plain.step(dt)
+        sa.pop("wall_time_ns"); sb.pop("wall_time_ns")  # host clock
+        assert sa == sb, (k, sa, sb)
+    assert np.array_equal(ring.copy_m(), plain.copy_m())
+    ring.refresh_observables()
+    plain.refresh_observables()
+    for o in (nf.OBS_H_EX, nf.OBS_H_DEMAG, nf.OBS_H_EFF):
+        assert np.array_equal(ring.copy_field(o), plain.copy_field(o)), o
+
