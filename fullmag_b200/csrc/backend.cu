@@ -212,12 +212,14 @@ struct Impl {
                 b.thr_x = lp * L2;
                 b.rsm_x = (size_t)(lp * TE) * sz;
                 ok &= cuda_ok(b, cudaFuncSetAttribute(k_xf_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_x), "attr xf_r");
-                ok &= cuda_ok(b, cudaFuncSetAttribute(k_xi_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_x), "attr xi_r");
+                b.rsm_xi = b.rsm_x + (size_t)L1 * L2 * sz;  // + the twiddle table
+                ok &= cuda_ok(b, cudaFuncSetAttribute(k_xi_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_xi), "attr xi_r");
                 // pipelined x forward for a uniform material with 16-byte rows
                 b.use_xpipe = false;
                 if (ok && !b.has_mask && !b.has_ms_map && !b.boundary_tier && (b.nx * sizeof(T)) % 16 == 0) {
                     const int RB = 2 * lp;
-                    const size_t smem = xpipe_region_bytes<L1, L2, T>(lp) + (size_t)2 * RB * b.nx * sizeof(T);
+                    const size_t smem = xpipe_region_bytes<L1, L2, T>(lp) + (size_t)2 * RB * b.nx * sizeof(T) +
+                                        (size_t)L1 * L2 * sizeof(C);
                     int occ = 0, sms = 148;
                     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.device);
                     if (smem <= 200 * 1024 &&
@@ -345,7 +347,7 @@ struct Impl {
             constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
             if constexpr (!(sizeof(T) == 8 && L1 > 32)) {
                 ProfScope p(b, "demag_x_inv");
-                k_xi_r<T, L1, L2><<<gx, b.thr_x, b.rsm_x, b.stream>>>(a);
+                k_xi_r<T, L1, L2><<<gx, b.thr_x, b.rsm_xi, b.stream>>>(a);
             }
         });
         return check_launch(b, "demag (register FFT)");

@@ -105,6 +105,7 @@ struct Backend {
     int yz_min_P = 1;             // FULLMAG_FDM_YZ_P: smallest cluster size tried
     size_t rsm_yz = 0;
     size_t rsm_x = 0, rsm_y = 0, rsm_yc = 0;
+    size_t rsm_xi = 0;            // x inverse: line regions + twiddle table
     bool zdirect = false;         // 3-D, nz <= 8: z convolution by direct summation (k_zd)
     int grid_zd = 0;              // its persistent grid (resident blocks x SMs)
     size_t rsm_zd = 0;

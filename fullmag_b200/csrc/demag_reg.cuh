@@ -93,7 +93,8 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
 // cp.async while the current group is transformed (double buffer, one commit
 // group per chunk), so the row loads no longer stall the FFT.  The transform
 // and the transposed store are those of xf_body.
-// Shared memory: lines_x line regions (TE complex each), then 2 x RB nx reals.
+// Shared memory: lines_x line regions (TE complex each), 2 x RB nx reals, then
+// the Lx twiddles of fft4step (2 x RB nx reals keep them 16-byte aligned).
 // ---------------------------------------------------------------------------
 
 template <int L1, int L2, typename T>
@@ -111,6 +112,9 @@ __global__ void __launch_bounds__(256) k_xf_pipe(DemagArgs<T> a, int ngroups) {
     C *region = reinterpret_cast<C *>(smem_raw);
     T *stage = reinterpret_cast<T *>(smem_raw + xpipe_region_bytes<L1, L2, T>(LP));
     const size_t stage_elems = (size_t)RB * nx;
+    // the 4-step twiddle table, copied once per (persistent) block
+    C *tws = reinterpret_cast<C *>(stage + 2 * stage_elems);
+    for (int k = threadIdx.x; k < L; k += blockDim.x) tws[k] = a.twxT[k];
     constexpr int PER = 16 / (int)sizeof(T);  // elements per 16-byte copy
     auto issue = [&](int g, int buf) {
         const int yb = g % nyb, cz = g / nyb, z = cz % nz, c = cz / nz;
@@ -142,7 +146,7 @@ __global__ void __launch_bounds__(256) k_xf_pipe(DemagArgs<T> a, int ngroups) {
             return v;
         };
         auto out = [&](int k, C v) { line[k] = v; };
-        fft4step<L1, L2, false, false, true, true>(t, a.twxT, line, in, out);
+        fft4step<L1, L2, false, false, true, true>(t, tws, line, in, out);
         __syncthreads();
         C *s1row = a.s1 + ((long long)c * nz + z) * nkx * ny;
         auto emit = [&](int k, int r) {
@@ -173,12 +177,14 @@ __global__ void __launch_bounds__(256) k_xf_pipe(DemagArgs<T> a, int ngroups) {
 // x inverse: gather A/B half spectra (transposed), form Z = A + iB on the full
 // circle, C2R, crop, 1/P, mask.  Same grid as k_xf_r.
 // ---------------------------------------------------------------------------
-template <typename T, int L1, int L2>
+// TWS: the twiddles were copied into shared memory after the line regions
+// (k_xi_r; the batched kernels read them from global memory).
+template <typename T, int L1, int L2, bool TWS = false>
 __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, int c, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = line_region<L1, L2>();
-    const C *tw = a.twxT;
     C *region = reinterpret_cast<C *>(smem_raw);
+    const C *tw = TWS ? region + a.lines_x * TE : a.twxT;
     const int LP = a.lines_x, RB = 2 * LP, nx = a.nx, ny = a.ny, nkx = a.nkx;
     const int y0 = bx * RB;
     // Z[k] = A[k] + i B[k] (k <= nx), Z[L-k] = conj(A[k]) + i conj(B[k]); DC and
@@ -247,10 +253,14 @@ __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, in
     fft4step<L1, L2, true, true, false>(t, tw, line, in, out);
 }
 
+// Shared memory: lines_x line regions, then the Lx twiddles.
 template <typename T, int L1, int L2>
 __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    xi_body<T, L1, L2>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+    cx<T> *tws = reinterpret_cast<cx<T> *>(smem_raw) + a.lines_x * line_region<L1, L2>();
+    for (int k = threadIdx.x; k < L1 * L2; k += blockDim.x) tws[k] = a.twxT[k];
+    // the first barrier inside xi_body (after the gather) precedes every twiddle read
+    xi_body<T, L1, L2, true>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 // ---------------------------------------------------------------------------

@@ -195,7 +195,7 @@ extern "C" int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uin
     bool ok = true;
     // x passes: complex lines (row pairs) per block
     int thr_x = 0;
-    size_t smx = 0;
+    size_t smx = 0, smxi = 0;
     split_for(Lx, [&](auto l1, auto l2) {
         constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
         constexpr int TE = line_region<L1, L2>();
@@ -205,8 +205,9 @@ extern "C" int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uin
         a.lines_x = lp;
         thr_x = lp * L2;
         smx = (size_t)(lp * TE) * sz;
+        smxi = smx + (size_t)L1 * L2 * sz;  // the x inverse also holds the twiddle table
         ok &= cudaFuncSetAttribute(k_xf_r<double, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx) == cudaSuccess;
-        ok &= cudaFuncSetAttribute(k_xi_r<double, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx) == cudaSuccess;
+        ok &= cudaFuncSetAttribute(k_xi_r<double, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxi) == cudaSuccess;
     });
     int thr_y = 0;
     size_t smy = 0;
@@ -270,7 +271,7 @@ extern "C" int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uin
     }
     split_for(Lx, [&](auto l1, auto l2) {
         constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
-        k_xi_r<double, L1, L2><<<gx, thr_x, smx, st>>>(a);
+        k_xi_r<double, L1, L2><<<gx, thr_x, smxi, st>>>(a);
     });
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
