@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(256) k_xf_pipe(DemagArgs<T> a, int ngroups) {
 // ---------------------------------------------------------------------------
 // TWS: the twiddles were copied into shared memory after the line regions
 // (k_xi_r; the batched kernels read them from global memory).
-template <typename T, int L1, int L2, bool TWS = false>
+template <typename T, int L1, int L2, bool TWS = false, int U = 8>
 __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, int c, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = line_region<L1, L2>();
@@ -207,7 +207,6 @@ __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, in
     if (blockDim.x % RB == 0) {
         // fixed row per thread, warp-uniform trip count (the shuffle needs whole
         // warps); U independent loads in flight per thread before they are placed
-        constexpr int U = 8;
         const int r = threadIdx.x % RB, kstep = blockDim.x / RB, k0 = threadIdx.x / RB;
         const int y = y0 + r;
         const int iters = (nkx + kstep - 1) / kstep;
@@ -253,14 +252,18 @@ __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, in
     fft4step<L1, L2, true, true, false>(t, tw, line, in, out);
 }
 
-// Shared memory: lines_x line regions, then the Lx twiddles.
-template <typename T, int L1, int L2>
+// Shared memory: lines_x line regions, then the Lx twiddles.  U: gather loads
+// in flight per thread (xi_gather: measured at 512 x 512 x 8 with S1 out of
+// L2, FP32 U = 8 / 33: 57.4 / 52.3 us, FP64 U = 8 / 17: 102.7 / 94.8 us).
+template <typename T> __host__ __device__ constexpr int xi_gather() { return sizeof(T) == 4 ? 33 : 17; }
+
+template <typename T, int L1, int L2, int U = 8>
 __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *tws = reinterpret_cast<cx<T> *>(smem_raw) + a.lines_x * line_region<L1, L2>();
     for (int k = threadIdx.x; k < L1 * L2; k += blockDim.x) tws[k] = a.twxT[k];
     // the first barrier inside xi_body (after the gather) precedes every twiddle read
-    xi_body<T, L1, L2, true>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+    xi_body<T, L1, L2, true, U>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
