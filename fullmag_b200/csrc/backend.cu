@@ -252,7 +252,12 @@ struct Impl {
                     ok &= cuda_ok(b, cudaFuncSetAttribute(k_yc_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_yc), "attr yc_r");
                 } else {
                     constexpr int TE = tile_elems(L1, L2);
-                    const int lpb = std::max(1, 256 / L2);
+                    // lines per block: for 32-thread lines 6 (FP32) or 4 (FP64) lines,
+                    // measured at Ly = 1024 against 8 (FP32 -2 us per pass; FP64 8 lines
+                    // leave one 135 KB block per SM: 86.5 -> 74.5 us forward); at most
+                    // 68 KB of tiles per block otherwise
+                    int lpb = L2 == 32 ? (sizeof(T) == 8 ? 4 : 6) : std::max(1, 256 / L2);
+                    while (lpb > 1 && (size_t)(lpb * TE) * sz > 68 * 1024) lpb /= 2;
                     b.lines_y = lpb;
                     b.thr_y = lpb * L2;
                     b.rsm_y = (size_t)(lpb * TE) * sz;
