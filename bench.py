@@ -148,6 +148,7 @@ def kernel_bytes(name: str, g: dict, s: int) -> float:
         "demag_y_fwd": s1 + s2,
         "demag_z_conv": 2 * s2 + octant,
         "demag_z_direct": 2 * s2 + ztable,
+        "demag_yzy": 2 * s1 + ztable,  # y forward + z + y inverse of a kx plane in shared memory
         "demag_y_inv": s2 + s1,
         "demag_x_inv": s1 + 3 * n * s,
         "stage_combine": 9 * n * s,

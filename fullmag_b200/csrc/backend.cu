@@ -24,6 +24,7 @@
 #include "demag.cuh"
 #include "demag_reg.cuh"
 #include "demag_yz.hpp"
+#include "demag_yzy.hpp"
 #include "newell_host.hpp"
 #include "stages.cuh"
 #include "adjoint.cuh"
@@ -280,6 +281,9 @@ struct Impl {
                 b.rsm_zd = smem;
             });
         }
+        b.use_yzy = false;
+        if constexpr (sizeof(T) == 4)
+            if (ok && b.zdirect) ok &= yzy_configure(b);
         return ok;
     }
 
@@ -308,6 +312,11 @@ struct Impl {
         } else if (b.use_yz) {
             ProfScope p(b, "demag_yz");
             if (!yz_launch(b, a)) return false;
+        } else if (b.use_yzy) {
+            if constexpr (sizeof(T) == 4) {
+                ProfScope p(b, "demag_yzy");
+                if (!yzy_launch(b, a)) return false;
+            }
         } else {
             const long long lines = 3LL * b.nz * b.nkx;
             const unsigned gy = (unsigned)((lines + b.lines_y - 1) / b.lines_y);
@@ -382,6 +391,7 @@ struct Impl {
         }
         b.use_reg = false;
         b.zdirect = false;
+        b.use_yzy = false;
         if (!b.last_error.empty()) return false;
         const int budget = 100 * 1024;
         const int sz = (int)sizeof(C);

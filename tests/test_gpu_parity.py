@@ -491,3 +491,34 @@ def test_stage_ring_matches_register_prefetch(monkeypatch, prec, integrator):
     for o in (nf.OBS_H_EX, nf.OBS_H_DEMAG, nf.OBS_H_EFF):
         assert np.array_equal(ring.copy_field(o), plain.copy_field(o)), o
 
+
+# FP32 grids whose kx plane (3 nz lines of Ly) fits in shared memory run the y
+# forward FFT, the direct z sum and the y inverse FFT in one kernel per kx plane
+# (demag_yz y fused); the operations and their order are those of the three
+# split kernels (FULLMAG_FDM_YZY=off), so fields and trajectories must agree
+# bit for bit, and both must match the oracle.
+@pytest.mark.parametrize("cells", [(16, 128, 8), (16, 256, 5), (8, 512, 8), (4, 512, 7), (8, 1024, 3)])
+def test_fused_yzy_plane_pass_matches_split_bitwise(monkeypatch, cells):
+    for k in ("FULLMAG_FDM_FFT", "FULLMAG_FDM_YZ", "FULLMAG_FDM_ZCONV", "FULLMAG_FDM_YZY"):
+        monkeypatch.delenv(k, raising=False)
+    kw = dict(cells=cells, cell_size=(2e-9, 2.5e-9, 3e-9), alpha=0.3, h_ext=(1e4, -5e3, 2e4),
+              precision=nf.PRECISION_SINGLE, symmetric_kernel=True, seed=17)
+    fused, sim, _ = make_pair(**kw)
+    monkeypatch.setenv("FULLMAG_FDM_YZY", "off")
+    split, _, _ = make_pair(**kw)
+    fused.set_profiling(True)
+    fused.refresh_observables()
+    names = set(fused.profile())
+    fused.set_profiling(False)
+    assert "demag_yzy" in names and "demag_z_direct" not in names, names
+    split.refresh_observables()
+    for o in (nf.OBS_H_DEMAG, nf.OBS_H_EFF):
+        assert np.array_equal(fused.copy_field(o), split.copy_field(o)), o
+    err = _field_errors(fused, sim.observe())
+    for k, v in err.items():
+        assert v <= 2e-6, (k, v)
+    for _ in range(3):
+        fused.step(2e-14)
+        split.step(2e-14)
+    assert np.array_equal(fused.copy_m(), split.copy_m())
+
