@@ -21,6 +21,13 @@ template <typename T> __host__ __device__ __forceinline__ cx<T> mk(T a, T b) {
 }
 template <typename C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
 template <typename C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && !defined(FM_SCALAR_COMPLEX_ADD)
+// FP32 pairs: one packed instruction (sm_100), each part rounded as the scalar
+// op, so results do not change.  A translation unit whose kernels measured
+// faster with the scalar pair defines FM_SCALAR_COMPLEX_ADD before any include.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+#endif
 template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
     C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
 }

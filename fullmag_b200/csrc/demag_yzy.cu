@@ -16,6 +16,9 @@
 // result is bitwise the split path's.  Shared memory: 3 nz rows (rounded up to
 // whole passes) of tile_elems(L1, L2) complex, each row also its line's 4-step
 // tile, then the Ly twiddles.  One block per SM at Ly = 1024, nz = 8 (206 KB).
+// measured at 512 x 512 x 8: 112 us with scalar complex adds, 117 us with the
+// packed FP32 pair (the x passes gain from the packed form)
+#define FM_SCALAR_COMPLEX_ADD
 #include <cmath>
 #include <cstdlib>
 #include <string>
