@@ -282,8 +282,7 @@ struct Impl {
             });
         }
         b.use_yzy = false;
-        if constexpr (sizeof(T) == 4)
-            if (ok && b.zdirect) ok &= yzy_configure(b);
+        if (ok && b.zdirect) ok &= yzy_configure<T>(b);
         return ok;
     }
 
@@ -313,10 +312,8 @@ struct Impl {
             ProfScope p(b, "demag_yz");
             if (!yz_launch(b, a)) return false;
         } else if (b.use_yzy) {
-            if constexpr (sizeof(T) == 4) {
-                ProfScope p(b, "demag_yzy");
-                if (!yzy_launch(b, a)) return false;
-            }
+            ProfScope p(b, "demag_yzy");
+            if (!yzy_launch(b, a)) return false;
         } else {
             const long long lines = 3LL * b.nz * b.nkx;
             const unsigned gy = (unsigned)((lines + b.lines_y - 1) / b.lines_y);

@@ -492,17 +492,27 @@ def test_stage_ring_matches_register_prefetch(monkeypatch, prec, integrator):
         assert np.array_equal(ring.copy_field(o), plain.copy_field(o)), o
 
 
-# FP32 grids whose kx plane (3 nz lines of Ly) fits in shared memory run the y
-# forward FFT, the direct z sum and the y inverse FFT in one kernel per kx plane
-# (demag_yz y fused); the operations and their order are those of the three
-# split kernels (FULLMAG_FDM_YZY=off), so fields and trajectories must agree
-# bit for bit, and both must match the oracle.
-@pytest.mark.parametrize("cells", [(16, 128, 8), (16, 256, 5), (8, 512, 8), (4, 512, 7), (8, 1024, 3)])
-def test_fused_yzy_plane_pass_matches_split_bitwise(monkeypatch, cells):
-    for k in ("FULLMAG_FDM_FFT", "FULLMAG_FDM_YZ", "FULLMAG_FDM_ZCONV", "FULLMAG_FDM_YZY"):
+# Grids with the direct z table and Ly = 2 ny in 256..1024 run the y forward
+# FFT, the direct z sum and the y inverse FFT in one kernel per kx plane, the
+# plane's lines spread over a cluster of P CTAs (distributed shared memory).
+# The operations and their order are those of the three split kernels
+# (FULLMAG_FDM_YZY=off), so fields and trajectories must agree bit for bit, and
+# both must match the oracle.  P = 0: the size the library picks (FP32; FP64
+# runs fused only on request); 1, 2, 4, 8 forced with FULLMAG_FDM_YZY_P.
+_YZY_CASES = [(c, prec, 0 if prec == nf.PRECISION_SINGLE else 8)
+              for c in [(16, 128, 8), (16, 256, 5), (8, 512, 8), (4, 512, 7), (16, 512, 3)]
+              for prec in (nf.PRECISION_SINGLE, nf.PRECISION_DOUBLE)]
+_YZY_CASES += [((16, 256, 5), prec, P) for prec in (nf.PRECISION_SINGLE, nf.PRECISION_DOUBLE) for P in (1, 2, 4, 8)]
+
+
+@pytest.mark.parametrize("cells,prec,P", _YZY_CASES)
+def test_fused_yzy_plane_pass_matches_split_bitwise(monkeypatch, cells, prec, P):
+    for k in ("FULLMAG_FDM_FFT", "FULLMAG_FDM_YZ", "FULLMAG_FDM_ZCONV", "FULLMAG_FDM_YZY", "FULLMAG_FDM_YZY_P"):
         monkeypatch.delenv(k, raising=False)
+    if P:
+        monkeypatch.setenv("FULLMAG_FDM_YZY_P", str(P))
     kw = dict(cells=cells, cell_size=(2e-9, 2.5e-9, 3e-9), alpha=0.3, h_ext=(1e4, -5e3, 2e4),
-              precision=nf.PRECISION_SINGLE, symmetric_kernel=True, seed=17)
+              precision=prec, symmetric_kernel=True, seed=17)
     fused, sim, _ = make_pair(**kw)
     monkeypatch.setenv("FULLMAG_FDM_YZY", "off")
     split, _, _ = make_pair(**kw)
@@ -515,10 +525,10 @@ def test_fused_yzy_plane_pass_matches_split_bitwise(monkeypatch, cells):
     for o in (nf.OBS_H_DEMAG, nf.OBS_H_EFF):
         assert np.array_equal(fused.copy_field(o), split.copy_field(o)), o
     err = _field_errors(fused, sim.observe())
+    tol = 1e-13 if prec == nf.PRECISION_DOUBLE else 2e-6
     for k, v in err.items():
-        assert v <= 2e-6, (k, v)
+        assert v <= tol, (k, v)
     for _ in range(3):
         fused.step(2e-14)
         split.step(2e-14)
     assert np.array_equal(fused.copy_m(), split.copy_m())
-
