@@ -43,24 +43,38 @@ namespace fm {
 
 // lines owned by one CTA of a P-CTA cluster
 template <int NZ, int P> __host__ __device__ constexpr int yzy_nlh() { return (3 * NZ + P - 1) / P; }
+// lines per FFT pass: FP32 CTAs of at most 192 threads (168 registers each, so
+// that two CTAs of 107 KB fit per SM), FP64 at most 384
+template <typename T, int L2, int NZ, int P> __host__ __device__ constexpr int yzy_lpp() {
+    return yzy_nlh<NZ, P>() * L2 <= (sizeof(T) == 4 ? 192 : 384) ? yzy_nlh<NZ, P>() : (sizeof(T) == 4 ? 192 : 384) / L2;
+}
+// rows: the owned lines rounded up to whole passes (the idle line groups of a
+// last, partial pass use their own rows as 4-step scratch)
+template <typename T, int L2, int NZ, int P> __host__ __device__ constexpr int yzy_rows() {
+    return (yzy_nlh<NZ, P>() + yzy_lpp<T, L2, NZ, P>() - 1) / yzy_lpp<T, L2, NZ, P>() * yzy_lpp<T, L2, NZ, P>();
+}
 template <typename T, int L1, int L2, int NZ, int P>
 __host__ __device__ constexpr size_t yzy_smem() {
-    return ((size_t)yzy_nlh<NZ, P>() * tile_elems(L1, L2) + (size_t)L1 * L2) * sizeof(cx<T>);
+    return ((size_t)yzy_rows<T, L2, NZ, P>() * tile_elems(L1, L2) + (size_t)L1 * L2) * sizeof(cx<T>);
 }
 constexpr size_t kYzySmemMax = 227 * 1024;
 template <typename T, int L1, int L2, int NZ, int P>
 __host__ __device__ constexpr bool yzy_fits() {
-    return yzy_smem<T, L1, L2, NZ, P>() <= kYzySmemMax && yzy_nlh<NZ, P>() * L2 <= 384 &&
+    return yzy_smem<T, L1, L2, NZ, P>() <= kYzySmemMax &&
            (sizeof(T) == 4 || L1 <= 32);  // FP64 4-step lines: 32 values per thread at most
+}
+template <typename T, int L2, int NZ, int P> __host__ __device__ constexpr int yzy_threads() {
+    return yzy_lpp<T, L2, NZ, P>() * L2;
 }
 
 template <typename T, int L1, int L2, int NZ, int P>
-__global__ void __launch_bounds__(yzy_nlh<NZ, P>() * L2) k_yzy(DemagArgs<T> a) {
+__global__ void __launch_bounds__(yzy_threads<T, L2, NZ, P>()) k_yzy(DemagArgs<T> a) {
     using C = cx<T>;
-    constexpr int L = L1 * L2, TE = tile_elems(L1, L2), NL = 3 * NZ, NLH = yzy_nlh<NZ, P>(), BT = NLH * L2;
+    constexpr int L = L1 * L2, TE = tile_elems(L1, L2), NL = 3 * NZ, NLH = yzy_nlh<NZ, P>();
+    constexpr int LPP = yzy_lpp<T, L2, NZ, P>(), ROWS = yzy_rows<T, L2, NZ, P>(), BT = LPP * L2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *S = reinterpret_cast<C *>(smem_raw);
-    C *tws = S + NLH * TE;
+    C *tws = S + ROWS * TE;
     const int h = P > 1 ? (int)cg::this_cluster().block_rank() : 0;
     auto cluster_sync = [&]() {
         if constexpr (P > 1) cg::this_cluster().sync();
@@ -70,12 +84,14 @@ __global__ void __launch_bounds__(yzy_nlh<NZ, P>() * L2) k_yzy(DemagArgs<T> a) {
     __syncthreads();  // fft4step reads twiddles before its first barrier
     const int kx = blockIdx.x / P, nkx = a.nkx, ny = a.ny;
     const int qg = threadIdx.x / L2, t = threadIdx.x - qg * L2;
-    const int q = h * NLH + qg;  // line q = c nz + z
-    const bool valid = q < NL;   // the last CTA may own fewer lines: its spare rows are scratch
-    C *line1 = a.s1 + ((long long)(valid ? q : 0) * nkx + kx) * ny;  // S1 [c][z][kx][y]
-    C *row = S + qg * TE;
-    // 1. forward y: inputs y < ny (= L/2; the upper half is the zero padding)
-    {
+    // 1. forward y, LPP lines per pass: inputs y < ny (= L/2; the upper half is the
+    // zero padding).  Every thread takes part in every pass (fft4step has barriers).
+#pragma unroll 1
+    for (int r0 = 0; r0 < ROWS; r0 += LPP) {
+        const int lr = r0 + qg, q = h * NLH + lr;  // local row, line q = c nz + z
+        const bool valid = lr < NLH && q < NL;     // spare rows are scratch
+        const C *line1 = a.s1 + ((long long)(valid ? q : 0) * nkx + kx) * ny;  // S1 [c][z][kx][y]
+        C *row = S + lr * TE;
         auto in1 = [&](int j) -> C { return valid ? line1[j] : mk<T>(0, 0); };
         auto out1 = [&](int k, C v) { row[k] = v; };
         fft4step<L1, L2, false, false, true, true>(t, tws, row, in1, out1);
@@ -149,7 +165,12 @@ __global__ void __launch_bounds__(yzy_nlh<NZ, P>() * L2) k_yzy(DemagArgs<T> a) {
     }
     cluster_sync();  // after this no CTA touches another's shared memory
     // 3. inverse y, keep y < ny
-    {
+#pragma unroll 1
+    for (int r0 = 0; r0 < ROWS; r0 += LPP) {
+        const int lr = r0 + qg, q = h * NLH + lr;
+        const bool valid = lr < NLH && q < NL;
+        C *line1 = a.s1 + ((long long)(valid ? q : 0) * nkx + kx) * ny;
+        C *row = S + lr * TE;
         auto in3 = [&](int j) -> C { return row[j]; };
         auto out3 = [&](int k, C v) { if (valid && k < ny) line1[k] = v; };
         fft4step<L1, L2, true, true, false>(t, tws, row, in3, out3);
@@ -215,7 +236,7 @@ cudaLaunchConfig_t yzy_config(const Backend &b, cudaLaunchAttribute *attr) {
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.gridDim = dim3((unsigned)(b.nkx * P));
-    cfg.blockDim = dim3((unsigned)(yzy_nlh<NZ, P>() * L2));
+    cfg.blockDim = dim3((unsigned)yzy_threads<T, L2, NZ, P>());
     cfg.dynamicSmemBytes = yzy_smem<T, L1, L2, NZ, P>();
     cfg.stream = b.stream;
     cfg.attrs = attr;
@@ -246,7 +267,10 @@ bool yzy_configure_t(Backend &b) {
                     constexpr size_t smem = yzy_smem<T, L1, L2, NZ, PP>();
                     if (!want && PP < 8 && smem > kYzySmemMax / 2) return;  // one CTA per SM: try a larger cluster
                     auto kern = k_yzy<T, L1, L2, NZ, PP>;
-                    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+                    // the largest shared-memory carveout, so that two CTAs fit per SM
+                    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+                        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                             (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess) {
                         cudaGetLastError();
                         return;
                     }
