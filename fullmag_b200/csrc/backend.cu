@@ -214,7 +214,11 @@ struct Impl {
                 b.rsm_x = (size_t)(lp * TE) * sz;
                 ok &= cuda_ok(b, cudaFuncSetAttribute(k_xf_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_x), "attr xf_r");
                 b.rsm_xi = b.rsm_x + (size_t)L1 * L2 * sz;  // + the twiddle table
-                ok &= cuda_ok(b, cudaFuncSetAttribute(k_xi_r<T, L1, L2, xi_gather<T>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_xi), "attr xi_r");
+                // even ny: the pair gather (both rows of a line pair per load)
+                b.xi_pair = b.ny % 2 == 0;
+                ok &= cuda_ok(b, cudaFuncSetAttribute(b.xi_pair ? k_xi_r<T, L1, L2, xi_gather_pair<T>(), true>
+                                                                : k_xi_r<T, L1, L2, xi_gather<T>(), false>,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_xi), "attr xi_r");
                 // pipelined x forward for a uniform material with 16-byte rows
                 b.use_xpipe = false;
                 if (ok && !b.has_mask && !b.has_ms_map && !b.boundary_tier && (b.nx * sizeof(T)) % 16 == 0) {
@@ -358,7 +362,10 @@ struct Impl {
             constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
             if constexpr (!(sizeof(T) == 8 && L1 > 32)) {
                 ProfScope p(b, "demag_x_inv");
-                k_xi_r<T, L1, L2, xi_gather<T>()><<<gx, b.thr_x, b.rsm_xi, b.stream>>>(a);
+                if (b.xi_pair)
+                    k_xi_r<T, L1, L2, xi_gather_pair<T>(), true><<<gx, b.thr_x, b.rsm_xi, b.stream>>>(a);
+                else
+                    k_xi_r<T, L1, L2, xi_gather<T>(), false><<<gx, b.thr_x, b.rsm_xi, b.stream>>>(a);
             }
         });
         return check_launch(b, "demag (register FFT)");

@@ -106,6 +106,7 @@ struct Backend {
     size_t rsm_yz = 0;
     size_t rsm_x = 0, rsm_y = 0, rsm_yc = 0;
     size_t rsm_xi = 0;            // x inverse: line regions + twiddle table
+    bool xi_pair = false;         // x inverse gathers row pairs (ny even)
     bool zdirect = false;         // 3-D, nz <= 8: z convolution by direct summation (k_zd)
     bool use_yzy = false;         // y forward + direct z + y inverse fused per kx plane (k_yzy)
     int yzy_P = 0;                // its cluster size (CTAs per plane)

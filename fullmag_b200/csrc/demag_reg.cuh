@@ -179,7 +179,10 @@ __global__ void __launch_bounds__(256) k_xf_pipe(DemagArgs<T> a, int ngroups) {
 // ---------------------------------------------------------------------------
 // TWS: the twiddles were copied into shared memory after the line regions
 // (k_xi_r; the batched kernels read them from global memory).
-template <typename T, int L1, int L2, bool TWS = false, int U = 8>
+// PAIR (ny even): a thread loads both rows of its line pair at one kx (adjacent
+// in S1) and writes Z[k], Z[L - k] itself, instead of the row-per-thread gather
+// whose pairs meet by shuffles; same values, no idle lanes.
+template <typename T, int L1, int L2, bool TWS = false, int U = 8, bool PAIR = false>
 __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, int c, unsigned char *smem_raw) {
     using C = cx<T>;
     constexpr int L = L1 * L2, TE = line_region<L1, L2>();
@@ -204,7 +207,47 @@ __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, in
             }
         }
     };
-    if (blockDim.x % RB == 0) {
+    if (PAIR && blockDim.x % LP == 0) {
+        const int qq = threadIdx.x % LP, kstep = blockDim.x / LP, k0 = threadIdx.x / LP;
+        const int ya = y0 + 2 * qq;  // ny even: ya < ny implies ya + 1 < ny
+        const bool rows = ya < ny;
+        const int iters = (nkx + kstep - 1) / kstep;
+        C *ln = region + qq * TE;
+        for (int it0 = 0; it0 < iters; it0 += U) {
+            C va[U], vb[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k = k0 + (it0 + u) * kstep;
+                if (k < nkx && rows) {
+                    const C *p = s1row + (long long)k * ny + ya;
+                    if constexpr (sizeof(C) == 8) {
+                        const float4 v = *reinterpret_cast<const float4 *>(p);  // 16-byte aligned: ya, ny even
+                        va[u] = mk<T>(v.x, v.y);
+                        vb[u] = mk<T>(v.z, v.w);
+                    } else {
+                        va[u] = p[0];
+                        vb[u] = p[1];
+                    }
+                } else {
+                    va[u] = mk<T>(0, 0);
+                    vb[u] = mk<T>(0, 0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k = k0 + (it0 + u) * kstep;
+                if (k < nkx) {
+                    const C A = va[u], B = vb[u];
+                    if (k == 0 || k == L / 2) {
+                        ln[k] = mk<T>(A.x, B.x);
+                    } else {
+                        ln[k] = mk<T>(A.x - B.y, A.y + B.x);
+                        ln[L - k] = mk<T>(A.x + B.y, -A.y + B.x);
+                    }
+                }
+            }
+        }
+    } else if (blockDim.x % RB == 0) {
         // fixed row per thread, warp-uniform trip count (the shuffle needs whole
         // warps); U independent loads in flight per thread before they are placed
         const int r = threadIdx.x % RB, kstep = blockDim.x / RB, k0 = threadIdx.x / RB;
@@ -243,8 +286,16 @@ __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, in
     T *hc = a.hd + (long long)c * a.n;
     const long long rowa = ((long long)z * ny + ya) * nx, rowb = rowa + nx;
     auto in = [&](int j) -> C { return line[j]; };
+    // no mask and no Ms map: every cell is active when Ms > 0 (cell_active's answer)
+    const bool uniform = !a.mask && !a.ms_map;
+    const bool uni_on = a.ms > 0.0;
     auto out = [&](int k, C v) {
         if (k >= nx) return;
+        if (uniform) {
+            if (ya < ny) hc[rowa + k] = uni_on ? v.x * nrm : T(0);
+            if (yb < ny) hc[rowb + k] = uni_on ? v.y * nrm : T(0);
+            return;
+        }
         double msi;
         if (ya < ny) hc[rowa + k] = cell_active(a, rowa + k, msi) ? v.x * nrm : T(0);
         if (yb < ny) hc[rowb + k] = cell_active(a, rowb + k, msi) ? v.y * nrm : T(0);
@@ -256,14 +307,16 @@ __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, in
 // in flight per thread (xi_gather: measured at 512 x 512 x 8 with S1 out of
 // L2, FP32 U = 8 / 33: 57.4 / 52.3 us, FP64 U = 8 / 17: 102.7 / 94.8 us).
 template <typename T> __host__ __device__ constexpr int xi_gather() { return sizeof(T) == 4 ? 33 : 17; }
+// pair gather (two rows per load): 17 / 9 load slots, one round at 513 kx
+template <typename T> __host__ __device__ constexpr int xi_gather_pair() { return sizeof(T) == 4 ? 17 : 9; }
 
-template <typename T, int L1, int L2, int U = 8>
+template <typename T, int L1, int L2, int U = 8, bool PAIR = false>
 __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *tws = reinterpret_cast<cx<T> *>(smem_raw) + a.lines_x * line_region<L1, L2>();
     for (int k = threadIdx.x; k < L1 * L2; k += blockDim.x) tws[k] = a.twxT[k];
     // the first barrier inside xi_body (after the gather) precedes every twiddle read
-    xi_body<T, L1, L2, true, U>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+    xi_body<T, L1, L2, true, U, PAIR>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
