@@ -70,7 +70,24 @@ __device__ __forceinline__ void xf_body(const DemagArgs<T> &a, int bx, int z, in
         else { o.x = T(0.5) * (zk.y + zm.y); o.y = T(-0.5) * (zk.x - zm.x); }
         s1row[(long long)k * ny + y] = o;
     };
-    if (blockDim.x % RB == 0) {
+    if (ny % 2 == 0 && blockDim.x % LP == 0) {
+        // a thread writes both rows of its line pair at one kx (adjacent in S1,
+        // one 16-byte store in FP32): Z[k] and Z[L - k] are read once
+        const int qq = threadIdx.x % LP, kstep = blockDim.x / LP, ya2 = y0 + 2 * qq;
+        if (ya2 < ny) {  // ny even: ya2 + 1 < ny as well
+            const C *ln = region + qq * TE;
+            for (int k = threadIdx.x / LP; k < nkx; k += kstep) {
+                const C zk = ln[k];
+                const C zm = ln[k == 0 ? 0 : L - k];
+                C o0, o1;
+                o0.x = T(0.5) * (zk.x + zm.x); o0.y = T(0.5) * (zk.y - zm.y);
+                o1.x = T(0.5) * (zk.y + zm.y); o1.y = T(-0.5) * (zk.x - zm.x);
+                C *d = s1row + (long long)k * ny + ya2;
+                if constexpr (sizeof(C) == 8) *reinterpret_cast<float4 *>(d) = make_float4(o0.x, o0.y, o1.x, o1.y);
+                else { d[0] = o0; d[1] = o1; }
+            }
+        }
+    } else if (blockDim.x % RB == 0) {
         // each thread keeps its row; k advances by blockDim / RB (no division in the loop)
         const int r = threadIdx.x % RB, kstep = blockDim.x / RB;
         for (int k = threadIdx.x / RB; k < nkx; k += kstep) emit(k, r);
@@ -160,7 +177,24 @@ __global__ void __launch_bounds__(256) k_xf_pipe(DemagArgs<T> a, int ngroups) {
             else { o.x = T(0.5) * (zk.y + zm.y); o.y = T(-0.5) * (zk.x - zm.x); }
             s1row[(long long)k * ny + y] = o;
         };
-        if (blockDim.x % RB == 0) {
+        if (ny % 2 == 0 && blockDim.x % LP == 0) {
+            // a thread writes both rows of its line pair at one kx (adjacent in S1,
+            // one 16-byte store in FP32): Z[k] and Z[L - k] are read once
+            const int qq = threadIdx.x % LP, kstep = blockDim.x / LP, ya2 = y0 + 2 * qq;
+            if (ya2 < ny) {  // ny even: ya2 + 1 < ny as well
+                const C *ln = region + qq * TE;
+                for (int k = threadIdx.x / LP; k < nkx; k += kstep) {
+                    const C zk = ln[k];
+                    const C zm = ln[k == 0 ? 0 : L - k];
+                    C o0, o1;
+                    o0.x = T(0.5) * (zk.x + zm.x); o0.y = T(0.5) * (zk.y - zm.y);
+                    o1.x = T(0.5) * (zk.y + zm.y); o1.y = T(-0.5) * (zk.x - zm.x);
+                    C *d = s1row + (long long)k * ny + ya2;
+                    if constexpr (sizeof(C) == 8) *reinterpret_cast<float4 *>(d) = make_float4(o0.x, o0.y, o1.x, o1.y);
+                    else { d[0] = o0; d[1] = o1; }
+                }
+            }
+        } else if (blockDim.x % RB == 0) {
             const int r = threadIdx.x % RB, kstep = blockDim.x / RB;
             for (int k = threadIdx.x / RB; k < nkx; k += kstep) emit(k, r);
         } else {
