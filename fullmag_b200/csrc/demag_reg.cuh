@@ -341,8 +341,8 @@ __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, in
 // in flight per thread (xi_gather: measured at 512 x 512 x 8 with S1 out of
 // L2, FP32 U = 8 / 33: 57.4 / 52.3 us, FP64 U = 8 / 17: 102.7 / 94.8 us).
 template <typename T> __host__ __device__ constexpr int xi_gather() { return sizeof(T) == 4 ? 33 : 17; }
-// pair gather (two rows per load): 17 / 9 load slots, one round at 513 kx
-template <typename T> __host__ __device__ constexpr int xi_gather_pair() { return sizeof(T) == 4 ? 17 : 9; }
+// pair gather (two rows per load): 17 load slots, one round at 513 kx
+template <typename T> __host__ __device__ constexpr int xi_gather_pair() { return 17; }
 
 template <typename T, int L1, int L2, int U = 8, bool PAIR = false>
 __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
