@@ -213,9 +213,10 @@ struct Impl {
                 b.thr_x = lp * L2;
                 b.rsm_x = (size_t)(lp * TE) * sz;
                 ok &= cuda_ok(b, cudaFuncSetAttribute(k_xf_r<T, L1, L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_x), "attr xf_r");
-                b.rsm_xi = b.rsm_x + (size_t)L1 * L2 * sz;  // + the twiddle table
                 // even ny: the pair gather (both rows of a line pair per load)
                 b.xi_pair = b.ny % 2 == 0;
+                b.rsm_xi = (size_t)lp * (b.xi_pair ? xi_stride<T, L1, L2, true>() : xi_stride<T, L1, L2, false>()) * sz +
+                           (size_t)L1 * L2 * sz;  // line regions + the twiddle table
                 ok &= cuda_ok(b, cudaFuncSetAttribute(b.xi_pair ? k_xi_r<T, L1, L2, xi_gather_pair<T>(), true>
                                                                 : k_xi_r<T, L1, L2, xi_gather<T>(), false>,
                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.rsm_xi), "attr xi_r");

@@ -213,13 +213,22 @@ __global__ void __launch_bounds__(256) k_xf_pipe(DemagArgs<T> a, int ngroups) {
 // ---------------------------------------------------------------------------
 // TWS: the twiddles were copied into shared memory after the line regions
 // (k_xi_r; the batched kernels read them from global memory).
+// Line stride of the x inverse's shared regions.  With the pair gather a warp
+// writes 4 lines x 8 kx (FP32) or a quarter-warp 4 lines x 2 kx (FP64): a stride
+// of 4 mod 16 (FP32) or 2 mod 8 (FP64) complex elements puts each phase's writes
+// in distinct banks (line_region's 1 mod 16 made them collide).  Lines of 32
+// threads only: a warp then holds one line inside fft4step.
+template <typename T, int L1, int L2, bool PAIR> __host__ __device__ constexpr int xi_stride() {
+    return (PAIR && L2 == 32) ? line_region<L1, L2>() + (sizeof(T) == 8 ? 1 : 3) : line_region<L1, L2>();
+}
+
 // PAIR (ny even): a thread loads both rows of its line pair at one kx (adjacent
 // in S1) and writes Z[k], Z[L - k] itself, instead of the row-per-thread gather
 // whose pairs meet by shuffles; same values, no idle lanes.
 template <typename T, int L1, int L2, bool TWS = false, int U = 8, bool PAIR = false>
 __device__ __forceinline__ void xi_body(const DemagArgs<T> &a, int bx, int z, int c, unsigned char *smem_raw) {
     using C = cx<T>;
-    constexpr int L = L1 * L2, TE = line_region<L1, L2>();
+    constexpr int L = L1 * L2, TE = xi_stride<T, L1, L2, PAIR>();
     C *region = reinterpret_cast<C *>(smem_raw);
     const C *tw = TWS ? region + a.lines_x * TE : a.twxT;
     const int LP = a.lines_x, RB = 2 * LP, nx = a.nx, ny = a.ny, nkx = a.nkx;
@@ -347,7 +356,7 @@ template <typename T> __host__ __device__ constexpr int xi_gather_pair() { retur
 template <typename T, int L1, int L2, int U = 8, bool PAIR = false>
 __global__ void __launch_bounds__(256) k_xi_r(DemagArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<T> *tws = reinterpret_cast<cx<T> *>(smem_raw) + a.lines_x * line_region<L1, L2>();
+    cx<T> *tws = reinterpret_cast<cx<T> *>(smem_raw) + a.lines_x * xi_stride<T, L1, L2, PAIR>();
     for (int k = threadIdx.x; k < L1 * L2; k += blockDim.x) tws[k] = a.twxT[k];
     // the first barrier inside xi_body (after the gather) precedes every twiddle read
     xi_body<T, L1, L2, true, U, PAIR>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
