@@ -20,6 +20,21 @@ template <int L1, int L2> __host__ __device__ constexpr int line_region() {
     return (tile_elems(L1, L2) > L1 * L2 ? tile_elems(L1, L2) : L1 * L2) + 1;
 }
 
+// Line stride of the x passes whose threads each handle a pair of rows (the x
+// inverse's gather, the pipelined x forward's transposed store): a warp touches
+// 4 lines x 8 kx (FP32) or a quarter-warp 4 lines x 2 kx (FP64) at once, and a
+// stride of 4 mod 16 (FP32) or 2 mod 8 (FP64) complex elements puts each phase
+// in distinct banks (line_region's 1 mod 16 made them collide).  Lines of 32
+// threads only: a warp then holds one line inside fft4step.
+template <typename T, int L1, int L2> __host__ __device__ constexpr int pair_stride() {
+    return L2 == 32 ? line_region<L1, L2>() + (sizeof(T) == 8 ? 1 : 3) : line_region<L1, L2>();
+}
+// the pipelined x forward: padded in FP32 only (measured at 1024-point lines:
+// FP32 28.9 -> 26.9 us, FP64 57.5 -> 65.6 us with the pad)
+template <typename T, int L1, int L2> __host__ __device__ constexpr int xf_stride() {
+    return sizeof(T) == 4 ? pair_stride<T, L1, L2>() : line_region<L1, L2>();
+}
+
 // ---------------------------------------------------------------------------
 // x forward: pack Ms*m (two rows per complex line), R2C, transposed store.
 // block = lines_x line groups of L2 threads; grid (ceil(ny / 2 lines_x), nz, 3)
@@ -110,19 +125,19 @@ __global__ void __launch_bounds__(256) k_xf_r(DemagArgs<T> a) {
 // cp.async while the current group is transformed (double buffer, one commit
 // group per chunk), so the row loads no longer stall the FFT.  The transform
 // and the transposed store are those of xf_body.
-// Shared memory: lines_x line regions (TE complex each), 2 x RB nx reals, then
+// Shared memory: lines_x line regions (xf_stride complex each), 2 x RB nx reals, then
 // the Lx twiddles of fft4step (2 x RB nx reals keep them 16-byte aligned).
 // ---------------------------------------------------------------------------
 
 template <int L1, int L2, typename T>
 __host__ __device__ constexpr size_t xpipe_region_bytes(int lines) {
-    return ((size_t)lines * line_region<L1, L2>() * 2 * sizeof(T) + 15) / 16 * 16;
+    return ((size_t)lines * xf_stride<T, L1, L2>() * 2 * sizeof(T) + 15) / 16 * 16;
 }
 
 template <typename T, int L1, int L2>
 __global__ void __launch_bounds__(256) k_xf_pipe(DemagArgs<T> a, int ngroups) {
     using C = cx<T>;
-    constexpr int L = L1 * L2, TE = line_region<L1, L2>();
+    constexpr int L = L1 * L2, TE = xf_stride<T, L1, L2>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int LP = a.lines_x, RB = 2 * LP, nx = a.nx, ny = a.ny, nz = a.nz, nkx = a.nkx;
     const int nyb = (ny + RB - 1) / RB;
@@ -213,13 +228,9 @@ __global__ void __launch_bounds__(256) k_xf_pipe(DemagArgs<T> a, int ngroups) {
 // ---------------------------------------------------------------------------
 // TWS: the twiddles were copied into shared memory after the line regions
 // (k_xi_r; the batched kernels read them from global memory).
-// Line stride of the x inverse's shared regions.  With the pair gather a warp
-// writes 4 lines x 8 kx (FP32) or a quarter-warp 4 lines x 2 kx (FP64): a stride
-// of 4 mod 16 (FP32) or 2 mod 8 (FP64) complex elements puts each phase's writes
-// in distinct banks (line_region's 1 mod 16 made them collide).  Lines of 32
-// threads only: a warp then holds one line inside fft4step.
+// line stride of the x inverse's shared regions (pair_stride with the pair gather)
 template <typename T, int L1, int L2, bool PAIR> __host__ __device__ constexpr int xi_stride() {
-    return (PAIR && L2 == 32) ? line_region<L1, L2>() + (sizeof(T) == 8 ? 1 : 3) : line_region<L1, L2>();
+    return PAIR ? pair_stride<T, L1, L2>() : line_region<L1, L2>();
 }
 
 // PAIR (ny even): a thread loads both rows of its line pair at one kx (adjacent
