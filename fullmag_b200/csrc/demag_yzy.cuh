@@ -11,7 +11,8 @@
 //   2. cluster barrier; CTA h sums the direct z convolution of the ky columns
 //      [h Ly/P, (h + 1) Ly/P), reading each column's 3 nz values from the
 //      owners' rows (distributed shared memory for the other CTAs' lines) and
-//      writing the results back there, one output component at a time;
+//      writing the results back there (k_zd's loop, all three components at once;
+//      one component at a time measured 104.6 against 99.4 us at 512 x 512 x 8);
 //   3. cluster barrier; inverse y (fft4step) from the owned rows back into S1,
 //      keeping y < ny.
 // The sums are those of k_zd, in the same order per output, and the FFTs are
@@ -121,45 +122,36 @@ __global__ void __launch_bounds__(yzy_threads<T, L2, NZ, P>()) k_yzy(DemagArgs<T
                 const C v = cell(2 * NZ + z, ky);
                 mz[z] = mk<T>(v.y, -v.x);  // -i Mz
             }
-            // output component r: coefficients (on Mx, My, Mz') of offset +d; offset -d
-            // flips the entries odd in z.  Per output the operations and their order
-            // are k_zd's.
+            C hx[NZ], hy[NZ], hz[NZ];
 #pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                C hh[NZ];
+            for (int z = 0; z < NZ; ++z) { hx[z] = mk<T>(0, 0); hy[z] = mk<T>(0, 0); hz[z] = mk<T>(0, 0); }
+            // the loop of k_zd: per output, offsets d ascending, +d then -d
 #pragma unroll
-                for (int z = 0; z < NZ; ++z) hh[z] = mk<T>(0, 0);
+            for (int d = 0; d < NZ; ++d) {
+                const T *qd = tp + d * dstr;
+                const T cxx = qd[0], cyy = qd[tstr], czz = qd[2 * tstr], cxy = qd[3 * tstr] * sy;
+                const T cxz = d > 0 ? qd[4 * tstr] : T(0), cyz = d > 0 ? qd[5 * tstr] * sy : T(0);
 #pragma unroll
-                for (int d = 0; d < NZ; ++d) {
-                    const T *qd = tp + d * dstr;
-                    T c0, c1, c2;
-                    bool odd0, odd1, odd2;  // entries odd in z (sign flip at -d)
-                    if (r == 0) {
-                        c0 = qd[0]; c1 = qd[3 * tstr] * sy; c2 = d > 0 ? qd[4 * tstr] : T(0);
-                        odd0 = false; odd1 = false; odd2 = true;
-                    } else if (r == 1) {
-                        c0 = qd[3 * tstr] * sy; c1 = qd[tstr]; c2 = d > 0 ? qd[5 * tstr] * sy : T(0);
-                        odd0 = false; odd1 = false; odd2 = true;
-                    } else {
-                        const T cxz = d > 0 ? qd[4 * tstr] : T(0), cyz = d > 0 ? qd[5 * tstr] * sy : T(0);
-                        c0 = -cxz; c1 = -cyz; c2 = qd[2 * tstr];
-                        odd0 = true; odd1 = true; odd2 = false;
+                for (int z = 0; z + d < NZ; ++z) {
+                    {   // output z + d from input z (offset +d)
+                        const int o = z + d;
+                        zd_fma(hx[o], cxx, mx[z]); zd_fma(hx[o], cxy, my[z]); zd_fma(hx[o], cxz, mz[z]);
+                        zd_fma(hy[o], cxy, mx[z]); zd_fma(hy[o], cyy, my[z]); zd_fma(hy[o], cyz, mz[z]);
+                        zd_fma(hz[o], -cxz, mx[z]); zd_fma(hz[o], -cyz, my[z]); zd_fma(hz[o], czz, mz[z]);
                     }
-#pragma unroll
-                    for (int z = 0; z < NZ; ++z) {
-                        if (z - d >= 0) {
-                            zd_fma(hh[z], c0, mx[z - d]); zd_fma(hh[z], c1, my[z - d]); zd_fma(hh[z], c2, mz[z - d]);
-                        }
-                        if (d > 0 && z + d < NZ) {
-                            zd_fma(hh[z], odd0 ? -c0 : c0, mx[z + d]);
-                            zd_fma(hh[z], odd1 ? -c1 : c1, my[z + d]);
-                            zd_fma(hh[z], odd2 ? -c2 : c2, mz[z + d]);
-                        }
+                    if (d > 0) {  // output z from input z + d (offset -d: odd-in-z entries flip)
+                        const int i = z + d;
+                        zd_fma(hx[z], cxx, mx[i]); zd_fma(hx[z], cxy, my[i]); zd_fma(hx[z], -cxz, mz[i]);
+                        zd_fma(hy[z], cxy, mx[i]); zd_fma(hy[z], cyy, my[i]); zd_fma(hy[z], -cyz, mz[i]);
+                        zd_fma(hz[z], cxz, mx[i]); zd_fma(hz[z], cyz, my[i]); zd_fma(hz[z], czz, mz[i]);
                     }
                 }
+            }
 #pragma unroll
-                for (int z = 0; z < NZ; ++z)
-                    cell(r * NZ + z, ky) = r == 2 ? mk<T>(-hh[z].y, hh[z].x) : hh[z];  // Hz = i Hz'
+            for (int z = 0; z < NZ; ++z) {
+                cell(z, ky) = hx[z];
+                cell(NZ + z, ky) = hy[z];
+                cell(2 * NZ + z, ky) = mk<T>(-hz[z].y, hz[z].x);  // Hz = i Hz'
             }
         }
     }
