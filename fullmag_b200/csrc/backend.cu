@@ -601,11 +601,8 @@ struct Impl {
         return check_launch(b, "combine");
     }
 
-    static bool read_stats(Backend &b) {
-        if (!cuda_ok(b, cudaMemcpyAsync(b.h_out, b.d_out, NQ * sizeof(double), cudaMemcpyDeviceToHost, b.stream), "stats D2H"))
-            return false;
-        return cuda_ok(b, cudaStreamSynchronize(b.stream), "stats sync");
-    }
+    // the reducing kernel wrote the statistics into the mapped host buffer h_out
+    static bool read_stats(Backend &b) { return cuda_ok(b, cudaStreamSynchronize(b.stream), "stats sync"); }
 
     static void fill_stats(Backend &b, double dt, fullmag_fdm_step_stats *st) {
         const double *o = b.h_out;
@@ -1165,7 +1162,6 @@ bool backend_alloc(Backend &b) {
         b.red_blocks = (int)std::max(general, blocks(zb));  // partials of either stage grid
     }
     items.push_back({(void **)&b.partials, (size_t)NQ * b.red_blocks * 8});
-    items.push_back({(void **)&b.d_out, (size_t)NQ * 8 + 64});
     items.push_back({(void **)&b.counter, 64});
     size_t total = 0;
     for (auto &it : items) total += (it.bytes + 255) / 256 * 256;
@@ -1177,7 +1173,11 @@ bool backend_alloc(Backend &b) {
         p += (it.bytes + 255) / 256 * 256;
     }
     if (!cuda_ok(b, cudaMemsetAsync(b.arena, 0, total, b.stream), "arena memset")) return false;
-    if (!cuda_ok(b, cudaMallocHost((void **)&b.h_out, NQ * sizeof(double) + 64), "cudaMallocHost(stats)")) return false;
+    // step statistics: the last block of a reducing kernel writes them straight
+    // into this mapped pinned buffer, so a step ends with a stream sync, no copy
+    if (!cuda_ok(b, cudaHostAlloc((void **)&b.h_out, NQ * sizeof(double) + 64, cudaHostAllocMapped), "cudaHostAlloc(stats)"))
+        return false;
+    if (!cuda_ok(b, cudaHostGetDevicePointer((void **)&b.d_out, b.h_out, 0), "stats device pointer")) return false;
     return true;
 }
 

@@ -116,7 +116,7 @@ struct Backend {
     // ---- reductions ----
     int red_blocks = 0;
     double *partials = nullptr;
-    double *d_out = nullptr;
+    double *d_out = nullptr;      // device address of h_out (mapped pinned memory)
     unsigned *counter = nullptr;  // blocks finished in the reducing stage kernel
     double *h_out = nullptr;  // pinned, NQ doubles
 

@@ -397,6 +397,8 @@ class NativeFdmBackend:
             self._lib.fullmag_fdm_backend_destroy(h)
             raise RunError(err.decode())
         self._h = h
+        self._st = StepStats()
+        self._st_ref = C.byref(self._st)
 
     # -- lifecycle --
     def close(self) -> None:
@@ -428,8 +430,8 @@ class NativeFdmBackend:
 
     # -- stepping --
     def step(self, dt: float) -> dict:
-        st = StepStats()
-        self._check(self._lib.fullmag_fdm_backend_step(self._h, dt, C.byref(st)), "step")
+        st = self._st  # one statistics buffer per backend, filled by every call
+        self._check(self._lib.fullmag_fdm_backend_step(self._h, dt, self._st_ref), "step")
         return st.as_dict()
 
     def step_n(self, dt: float, n: int) -> dict:
