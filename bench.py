@@ -14,7 +14,9 @@ Reported (one JSON line on rank 0):
           every step) and the final copy of m to host, all inside the timed
           region;
   fp64    the plain FP64 path's cell-updates/s and the FP32/FP64 ratio;
-  max_dm  max|m_fp32 - m_fp64| after the workload's 2000 steps from the same m0;
+  accuracy  max|m_fp32 - m_fp64| from the same m0 at steps 10 ... 2000 (the
+          workload's length), each beside FP64's own change from one FP32
+          rounding of m0, and the last checkpoint with max|dm| <= 1e-5;
   roofline  the dominant kernel's algorithmic bytes per launch / its mean
           launch time (CUDA events) against the measured HBM copy bandwidth;
   cpu_baseline  the FP64 CPU port of the reference engine (oracle/) timed on
@@ -42,7 +44,7 @@ MU0 = 4.0 * np.pi * 1e-7
 WORKLOAD = dict(cells=(512, 512, 8), cell_size=(2e-9, 2e-9, 2e-9), ms=8.0e5, aex=1.3e-11,
                 alpha=0.5, gamma=2.211e5, b_mT=(10.0, 0.0, 0.0), seed=43, dt=5e-14)
 METRIC = "cell-updates/s FP32-mixed vs plain FP64, 1 B200, at max|dm|<=1e-5; HBM GB/s"
-ACCURACY_STEPS = 2000  # the workload's step count; max|dm| FP32-mixed vs FP64 is taken there
+ACCURACY_CHECKPOINTS = (10, 50, 100, 200, 500, 1000, 2000)  # up to the workload's 2000 steps
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -152,8 +154,8 @@ def kernel_bytes(name: str, g: dict, s: int) -> float:
         "demag_y_inv": s2 + s1,
         "demag_x_inv": s1 + 3 * n * s,
         "stage_combine": 9 * n * s,
-        "stage_heun_corr": 15 * n * s,
-        "stage_eval": 9 * n * s,
+        "stage_heun_corr": 15 * n * s,   # reads m_p, H_d, m0, k1; writes m
+        "stage_eval": 12 * n * s,        # reads m, H_d; writes k and the next predictor
         "reduce_finalize": 0,
     }
     return float(table.get(name, 0))
@@ -224,7 +226,7 @@ def run_ours(args):
 
     results = {}
     sampler_out = None
-    floor_dm = None
+    m_out_pinned = torch.empty(3 * n, dtype=torch.float64).pin_memory()
     for prec, tag in ((nf.PRECISION_DOUBLE, "fp64"), (nf.PRECISION_SINGLE, "fp32")):
         be = make(prec)
         stream = torch.cuda.ExternalStream(be.stream())
@@ -251,39 +253,33 @@ def run_ours(args):
         be.step_n(dt, K)
         prof = be.profile()
         be.set_profiling(False)
-        # end to end through the C ABI from host buffers
+        # end to end through the C ABI from host buffers: upload of m0 from pinned
+        # memory, K step calls (statistics read back every step), copy of m into
+        # a pinned host array; the three parts are also timed on their own
         barrier_sync()
-        m_host = np.empty(3 * n)
-        f0 = torch.cuda.Event(enable_timing=True)
-        f1 = torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
         be.upload_m(m0_pinned.numpy())
+        ev[1].record(stream)
         for _ in range(K):
             be.step(dt)
-        m_host[:] = be.copy_m()
-        f1.record(stream)
-        f1.synchronize()
+        ev[2].record(stream)
+        be.copy_m(out=m_out_pinned.numpy())
+        ev[3].record(stream)
+        ev[3].synchronize()
         barrier_sync()
-        ms_e2e = max_over_ranks(f0.elapsed_time(f1))
-        # accuracy run: the workload's full 2000 steps from m0
-        be.upload_m(m0)
-        be.step_n(dt, ACCURACY_STEPS)
-        m_acc = be.copy_m()
-        if tag == "fp64":
-            # sensitivity floor of the workload itself: FP64 from m0 rounded once to FP32
-            be.upload_m(m0.astype(np.float32).astype(np.float64))
-            be.step_n(dt, ACCURACY_STEPS)
-            floor_dm = float(np.abs(be.copy_m() - m_acc).max())
-        results[tag] = dict(ms=ms, prof=prof, ms_e2e=ms_e2e, m=m_acc,
-                            mem=be.memory_info()[0])
+        ms_e2e = max_over_ranks(ev[0].elapsed_time(ev[3]))
+        e2e_parts = {"upload_ms": ev[0].elapsed_time(ev[1]), "steps_ms": ev[1].elapsed_time(ev[2]),
+                     "download_ms": ev[2].elapsed_time(ev[3])}
+        results[tag] = dict(ms=ms, prof=prof, ms_e2e=ms_e2e, e2e_parts=e2e_parts, mem=be.memory_info()[0])
         be.close()
+    accuracy = accuracy_table(make, nf, m0, dt)
 
     s32 = 4
     cells_job = n * K * world
     v32 = cells_job / (results["fp32"]["ms"] * 1e-3)
     v64 = cells_job / (results["fp64"]["ms"] * 1e-3)
     e2e32 = cells_job / (results["fp32"]["ms_e2e"] * 1e-3)
-    max_dm = float(np.abs(results["fp32"]["m"] - results["fp64"]["m"]).max())
 
     peak, peak_kind = hbm_peak()
     prof = results["fp32"]["prof"]
@@ -331,10 +327,12 @@ def run_ours(args):
                        "l2": "working set > 126 MB L2 per step (no flush needed)"},
             "fp64": {"value": v64, "ms_per_step": results["fp64"]["ms"] / K,
                      "speedup_fp32_over_fp64": v32 / v64, "kernels": kernels64},
-            "max_dm_fp32_vs_fp64": max_dm, "max_dm_after_steps": ACCURACY_STEPS,
-            "fp64_sensitivity_to_one_fp32_rounding_of_m0": floor_dm,
+            "accuracy": accuracy,
             "e2e": {"value": e2e32, "unit": "cell-updates/s", "h2d_bytes_per_step": bi,
-                    "d2h_bytes_per_step": bo,
+                    "d2h_bytes_per_step": bo, "steps": K,
+                    **{k: round(v, 4) for k, v in results["fp32"]["e2e_parts"].items()},
+                    "fixed_ms": round(results["fp32"]["e2e_parts"]["upload_ms"]
+                                      + results["fp32"]["e2e_parts"]["download_ms"], 4),
                     "fp64_value": cells_job / (results["fp64"]["ms_e2e"] * 1e-3)},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
@@ -344,6 +342,8 @@ def run_ours(args):
                             if dom == "demag_yzy" else {})},
             "step_roofline": {"algorithmic_bytes_per_step": step_bytes,
                               "achieved_gbs": step_bytes / (results["fp32"]["ms"] / K * 1e-3) / 1e9,
+                              # as built: the bytes the kernels this design runs must move
+                              "frac": step_bytes / (results["fp32"]["ms"] / K * 1e-3) / 1e9 / peak,
                               # per cell-update model B_Heun = 2 (78 s + 6 s_k) + 27 s, s = s_k = 4
                               "model_bytes_per_cell_update": 2 * (78 * s32 + 6 * s32) + 27 * s32,
                               "model_achieved_gbs": (2 * (78 * s32 + 6 * s32) + 27 * s32) * (v32 / world) / 1e9,
@@ -359,6 +359,33 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def accuracy_table(make, nf, m0, dt):
+    """max|m_fp32 - m_fp64| along the workload's 2000 steps from the same m0,
+    each beside FP64's own sensitivity: FP64 started from m0 rounded once to
+    FP32.  Any FP32-stored state carries at least that rounding, so the floor
+    bounds what an FP32-mixed run can reach at that step."""
+    a64, a32, f64 = make(nf.PRECISION_DOUBLE), make(nf.PRECISION_SINGLE), make(nf.PRECISION_DOUBLE)
+    f64.upload_m(m0.astype(np.float32).astype(np.float64))
+    rows, done, last_ok = [], 0, 0
+    for k in ACCURACY_CHECKPOINTS:
+        for be in (a64, a32, f64):
+            be.step_n(dt, k - done)
+        done = k
+        m64 = a64.copy_m()
+        dm = float(np.abs(a32.copy_m() - m64).max())
+        fl = float(np.abs(f64.copy_m() - m64).max())
+        rows.append({"step": k, "max_dm_fp32_vs_fp64": dm, "fp64_one_fp32_rounding_of_m0": fl})
+    for r in rows:  # the gate holds up to the first checkpoint that misses it
+        if r["max_dm_fp32_vs_fp64"] > 1e-5:
+            break
+        last_ok = r["step"]
+    for be in (a64, a32, f64):
+        be.close()
+    return {"rows": rows, "last_checkpoint_with_max_dm_le_1e-5": last_ok,
+            "note": "FP32-mixed vs FP64 from the same m0; the floor column is FP64 vs FP64 with m0 "
+                    "rounded once to FP32, which no FP32-stored state can avoid"}
 
 
 # --------------------------------------------------------------------- CPU (oracle) legs

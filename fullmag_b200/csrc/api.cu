@@ -10,8 +10,9 @@
 //   - last_error(NULL) is "null handle".
 // Additional validation (reported through last_error, never silently
 // accepted): non-positive cell sizes or Ms, region ids >= 256, unknown
-// integrators, boundary tiers this library does not implement, spectra that are not
-// the real, even/odd Newell form, padded FFT lengths with prime factors > 7.
+// integrator or boundary-tier values, boundary tiers whose per-cell arrays are
+// missing or of the wrong length, spectra that are not the real, even/odd
+// Newell form, padded FFT lengths with prime factors > 7.
 #include <algorithm>
 #include <chrono>
 #include <cmath>

@@ -49,21 +49,26 @@ void put_error(char *buf, uint64_t len, const char *msg) {
     }
 }
 
-// Once per device, with that device current: resolve the array's device
-// address (the host-side symbol is only a stand-in) and fill this file's copy
-// of the radix-64 twiddle table.
+// With the device current: resolve the array's device address (the host-side
+// symbol is only a stand-in) on every call, which is cheap, and once per
+// device (again if the address changed) fill this file's copy of the radix-64
+// twiddle table.  The upload goes through the legacy default stream from
+// pageable memory, which may return before the data reach the device, and a
+// caller's non-blocking stream is not ordered after it: the device is
+// synchronised once here, before the first kernel can read the table.
 bool setup_device(int dev, unsigned char **out, char *err, uint64_t errlen) {
     std::lock_guard<std::mutex> lock(g_mu);
     DeviceSlot &s = g_slots[dev];
-    if (!s.ready) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_fft_scratch);
-        if (e != cudaSuccess) {
-            char m[256];
-            std::snprintf(m, sizeof(m), "cudaGetSymbolAddress(g_fft_scratch): %s", cudaGetErrorString(e));
-            put_error(err, errlen, m);
-            return false;
-        }
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_fft_scratch);
+    if (e != cudaSuccess) {
+        char m[256];
+        std::snprintf(m, sizeof(m), "cudaGetSymbolAddress(g_fft_scratch): %s", cudaGetErrorString(e));
+        put_error(err, errlen, m);
+        return false;
+    }
+    if (!s.ready || s.scratch != p) {
+        s.ready = false;
         double2 d[64];
         float2 f[64];
         for (int k = 0; k < 64; ++k) {
@@ -73,6 +78,7 @@ bool setup_device(int dev, unsigned char **out, char *err, uint64_t errlen) {
         }
         e = cudaMemcpyToSymbol(c_tw64d, d, sizeof(d));
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tw64f, f, sizeof(f));
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) {
             char m[256];
             std::snprintf(m, sizeof(m), "twiddle table upload: %s", cudaGetErrorString(e));
@@ -133,6 +139,12 @@ extern "C" int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uin
         put_error(error_out, error_out_len, "null pointer, empty grid or non-positive Ms");
         return FULLMAG_FDM_ERR_INVALID;
     }
+    // range first, so that the doubled lengths below cannot overflow
+    if (nx > 512 || ny > 512 || nz > 8) {
+        put_error(error_out, error_out_len,
+                  "grid not supported: 2nx and 2ny must be powers of two <= 1024 and 2nz <= 16 (or nz = 1)");
+        return FULLMAG_FDM_ERR_INVALID;
+    }
     const bool thin = thin_film_2d && nz == 1;
     const int Lx = 2 * (int)nx, Ly = 2 * (int)ny, Lz = thin ? 1 : 2 * (int)nz;
     if (!pow2(Lx) || !pow2(Ly) || Lx > 1024 || Ly > 1024 || (!thin && (!pow2(Lz) || Lz > 16))) {
@@ -162,6 +174,9 @@ extern "C" int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uin
     unsigned char *base = nullptr;
     if (!setup_device(dev, &base, error_out, error_out_len)) return FULLMAG_FDM_ERR_CUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // a launch error left by earlier, unrelated work is not this call's: clear
+    // it, so that the check after the launches reports only this call's own
+    (void)cudaGetLastError();
 
     C *p = reinterpret_cast<C *>(base);
     C *twx = p, *twy = twx + Lx, *twz = twy + Ly;

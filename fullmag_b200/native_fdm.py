@@ -462,8 +462,14 @@ class NativeFdmBackend:
         return {"dl_dms": gms, "dl_dh_ext": ge, "dl_dh_ac": ga, "dl_dm0": g0}
 
     # -- transfers --
-    def copy_field(self, observable: int, dtype=np.float64) -> np.ndarray:
-        out = np.zeros(3 * self.n, dtype=dtype)
+    def copy_field(self, observable: int, dtype=np.float64, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """AoS copy of a field.  `out`: a caller-owned contiguous array of 3N
+        elements of `dtype` to fill (pinned memory makes the device-to-host copy
+        run at full speed); otherwise a new array."""
+        if out is None:
+            out = np.empty(3 * self.n, dtype=dtype)
+        elif out.dtype != dtype or out.size != 3 * self.n or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"out must be a contiguous {np.dtype(dtype).name} array of {3 * self.n} elements")
         if dtype == np.float64:
             rc = self._lib.fullmag_fdm_backend_copy_field_f64(self._h, observable, out.ctypes.data_as(_dp), out.size)
         else:
@@ -472,8 +478,8 @@ class NativeFdmBackend:
         self._check(rc, "copy_field")
         return out
 
-    def copy_m(self) -> np.ndarray:
-        return self.copy_field(OBS_M)
+    def copy_m(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        return self.copy_field(OBS_M, out=out)
 
     def copy_preview(self, observable: int, preview: Tuple[int, int, int], z_origin: int = 0,
                      z_stride: int = 1, dtype=np.float64) -> np.ndarray:

@@ -44,8 +44,9 @@ typedef enum {
     FULLMAG_FDM_PRECISION_DOUBLE = 2,
 } fullmag_fdm_precision;
 
-/* Time integrators (fullmag_fdm.h:52-58).  This library implements HEUN and
- * DP45; ABM3, RK4 and RK23 are rejected at create time with ERR_INVALID. */
+/* Time integrators (fullmag_fdm.h:52-58).  All five are implemented, in both
+ * precisions: HEUN and DP45 (adaptive, FSAL) on the hot path, and ABM3, RK4
+ * and RK23 (adaptive) on the same fused stage kernels. */
 typedef enum {
     FULLMAG_FDM_INTEGRATOR_HEUN = 1,
     FULLMAG_FDM_INTEGRATOR_DP45 = 2,
@@ -69,8 +70,11 @@ typedef enum {
     FULLMAG_FDM_SNAPSHOT_SCALAR_F64 = 2,
 } fullmag_fdm_snapshot_scalar_type;
 
-/* Boundary-correction tier (fullmag_fdm.h:73-77).  Only NONE (binary mask)
- * is implemented; VOLUME and FULL are rejected with ERR_INVALID. */
+/* Boundary-correction tier (fullmag_fdm.h:73-77).  All three are implemented:
+ * NONE (binary mask), VOLUME (T0 face-link exchange and phi-weighted demag) and
+ * FULL (T1 ECB exchange stencil, phi-weighted demag and the sparse demag
+ * correction).  A tier whose per-cell arrays are missing or of the wrong length
+ * is rejected with ERR_INVALID instead of being skipped. */
 typedef enum {
     FULLMAG_FDM_BOUNDARY_NONE   = 0,
     FULLMAG_FDM_BOUNDARY_VOLUME = 1,

@@ -164,11 +164,14 @@ int fullmag_fdm_newell_spectra(uint32_t nx, uint32_t ny, uint32_t nz, double dx,
  * exits).  Larger grids are rejected with FULLMAG_FDM_ERR_INVALID and a message
  * giving the bytes needed.
  *
- * The first call on a device resolves the scratch array's device address and
- * fills the twiddle constants; make that first call outside any CUDA stream
- * capture.  All calls share the one scratch array: calls that overlap on the
- * GPU (different streams or threads without ordering) race.  Each call writes
- * every scratch element it reads, so nothing has to start at zero. */
+ * The first call on a device resolves the scratch array's device address,
+ * fills the twiddle constants and synchronises the device once; make that
+ * first call outside any CUDA stream capture.  The constants are not refilled
+ * after cudaDeviceReset (or any new primary context) on that device, so do not
+ * use this entry point across a device reset.  All calls share the one scratch
+ * array: calls that overlap on the GPU (different streams or threads without
+ * ordering) race.  Each call writes every scratch element it reads, so nothing
+ * has to start at zero. */
 int fullmag_fdm_demag_field_f64_noalloc(uint32_t nx, uint32_t ny, uint32_t nz,
                                         int thin_film_2d, const double *octant,
                                         const double *m, double ms, double *h,

@@ -114,8 +114,9 @@ def test_c1_sensitivity_floor_and_1000_steps():
     for k, g, f, graw in rows:
         print(f"C1 step {k:5d}: gpu-vs-oracle {g:.3e}  oracle per-step-ulp floor {f:.3e}  "
               f"gpu-vs-oracle(reference spectra) {graw:.3e}")
+    # measured: the GPU sits at about 0.4x the oracle's own per-step 1-ulp floor
     for k, g, f, _ in rows:
-        assert g <= max(100.0 * f, 1e-12), (k, g, f)
+        assert g <= max(2.0 * f, 1e-12), (k, g, f)
     assert rel(st["total_energy_joules"], r["e_total"]) <= 1e-3
 
 

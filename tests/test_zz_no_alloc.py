@@ -39,7 +39,9 @@ def _octant(spectra, nx, ny, nz, thin):
     return np.ascontiguousarray(np.stack(out))
 
 
-@pytest.mark.parametrize("cells,thin", [((64, 32, 1), True), ((32, 16, 4), False), ((16, 8, 8), False)])
+# nz = 1 thin (2-D y pass), and 3-D with 2nz = 2, 4, 8 and 16 (the z FFT pass at each length)
+@pytest.mark.parametrize("cells,thin", [((64, 32, 1), True), ((16, 16, 1), False), ((32, 16, 2), False),
+                                        ((32, 16, 4), False), ((16, 8, 8), False)])
 def test_noalloc_demag_matches_regular_entry_point(cells, thin):
     import torch
 
@@ -89,5 +91,9 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     assert rc == nf.ERR_INVALID
     assert b"at most" in err.value and b"bytes" in err.value
     rc = fn(12, 8, 1, 1, dummy.data_ptr(), dummy.data_ptr(), 8e5, dummy.data_ptr(), None,
+            err, len(err))
+    assert rc == nf.ERR_INVALID and b"powers of two" in err.value
+    # sizes far beyond the limits are rejected before any length is formed
+    rc = fn(0x80000000, 8, 1, 1, dummy.data_ptr(), dummy.data_ptr(), 8e5, dummy.data_ptr(), None,
             err, len(err))
     assert rc == nf.ERR_INVALID and b"powers of two" in err.value
