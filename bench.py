@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble (C4) measurement")
+    ap.add_argument("--no-c3", action="store_true", help="skip the large masked DP45 (C3) measurement")
+    ap.add_argument("--no-c5", action="store_true", help="skip the adjoint (C5) timing")
     ap.add_argument("--kernels-only", action="store_true",
                     help="FP32-mixed warm-up + K timed steps only (for profiler runs)")
     return ap.parse_args()
@@ -154,6 +156,11 @@ def kernel_bytes(name: str, g: dict, s: int) -> float:
         "demag_y_inv": s2 + s1,
         "demag_x_inv": s1 + 3 * n * s,
         "stage_combine": 9 * n * s,
+        # fused row pass: S1 in and out; RHS: reads m, writes k and the predictor;
+        # corrector: reads m_p, m0, k1, writes m (H_d stays in shared memory)
+        "row_eval": 2 * s1 + 9 * n * s,
+        "row_heun_corr": 2 * s1 + 12 * n * s,
+        "row_x_fwd": 3 * n * s + s1,
         "stage_heun_corr": 15 * n * s,   # reads m_p, H_d, m0, k1; writes m
         "stage_eval": 12 * n * s,        # reads m, H_d; writes k and the next predictor
         "reduce_finalize": 0,
@@ -310,6 +317,12 @@ def run_ours(args):
     batch = None
     if not args.no_batch:
         batch = batch_ensemble_sample()
+    c3 = None
+    if not args.no_c3:
+        c3 = c3_masked_dp45_sample()
+    c5 = None
+    if not args.no_c5:
+        c5 = c5_adjoint_sample()
 
     if rank == 0:
         bi = 3 * n * 8 / K
@@ -354,6 +367,8 @@ def run_ours(args):
             "clocks": sampler_out,
             "cpu_baseline": cpu,
             "c4_batch": batch,
+            "c3_masked_dp45": c3,
+            "c5_adjoint": c5,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -397,6 +412,139 @@ def _oracle_problem(nx, ny, nz):
                         gamma=W["gamma"], h_ext=h)
 
 
+def c3_mask(nx=1024, ny=1024, nz=16, d=2e-9, r_out=1e-6, r_in=150e-9):
+    """C3 geometry: a disk of radius 1 um with a centred hole of radius 150 nm
+    (300 nm diameter), cell-centre test; Ms = 0 outside."""
+    x = (np.arange(nx) + 0.5) * d - nx * d / 2
+    y = (np.arange(ny) + 0.5) * d - ny * d / 2
+    X, Y = np.meshgrid(x, y)
+    r2 = X ** 2 + Y ** 2
+    m2 = (r2 <= r_out ** 2) & (r2 > r_in ** 2)
+    return np.repeat(m2[None], nz, axis=0).astype(np.uint8).reshape(-1)
+
+
+def c3_masked_dp45_sample(warm=3, steps=10):
+    """C3 on this GPU: 1024 x 1024 x 16 masked film, FP32-mixed DP45 at
+    max_error 1e-5 from the planner generator's m0 (seed 44), the suggested dt
+    fed back.  `warm` accepted steps untimed, then `steps` accepted steps timed
+    with CUDA events on the library's stream, then the same window again with
+    per-kernel events.  A window this short starts from the random m0, where
+    the accepted dt is smallest, so the time to 5 ns is an upper bound."""
+    import torch
+    from fullmag_b200 import native_fdm as nf
+    nx, ny, nz, d = 1024, 1024, 16, 2e-9
+    n = nx * ny * nz
+    mask = c3_mask(nx, ny, nz, d)
+    active = int(mask.sum())
+    m0 = nf.random_unit_vectors(44, n)
+    t0 = time.time()
+    plan = nf.FdmPlan(cells=(nx, ny, nz), cell_size=(d, d, d), initial_magnetization=m0,
+                      saturation_magnetisation=8e5, exchange_stiffness=1.3e-11, damping=0.1,
+                      gyromagnetic_ratio=2.211e5, precision=nf.PRECISION_SINGLE, integrator=nf.DP45,
+                      external_field=(0.0, 30e-3 / MU0, 0.0), active_mask=mask,
+                      adaptive=(1e-5, 1e-18, 1e-10, 0.8), demag_source=nf.DEMAG_NEWELL)
+    be = nf.NativeFdmBackend(plan)
+    t_create = time.time() - t0
+    stream = torch.cuda.ExternalStream(be.stream())
+    dt = 1e-13
+    for _ in range(warm):
+        dt = be.step(dt)["suggested_next_dt"]
+
+    def window(prof):
+        nonlocal dt
+        if prof:
+            be.set_profiling(True)
+            be.profile_reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dts = []
+        e0.record(stream)
+        for _ in range(steps):
+            st = be.step(dt)
+            dts.append(st["dt_seconds"])
+            dt = st["suggested_next_dt"]
+        e1.record(stream)
+        e1.synchronize()
+        out = (e0.elapsed_time(e1), dts, st)
+        if prof:
+            out = out + (be.profile(),)
+            be.set_profiling(False)
+        return out
+
+    ms, dts, st, *_ = window(False)
+    _, _, _, prof = window(True)
+    be.close()
+    s = 4
+    D = 78 * s + 6 * s            # bytes per cell of one 3-D demag evaluation (5 passes, octant spectra)
+    model = 6 * D + 168 * s       # per cell-update of an accepted DP45 step (FSAL, 6 evaluations)
+    peak, peak_kind = hbm_peak()
+    v_all = n * steps / (ms * 1e-3)
+    attempts = prof.get("stage_dp45_last", (0.0, steps))[1]
+    kern = {k: {"ms_per_launch": round(v[0] / v[1], 5), "launches": v[1],
+                "share": round(v[0] / sum(x[0] for x in prof.values()), 4)} for k, v in sorted(prof.items())}
+    mean_dt = float(np.mean(dts))
+    return {"workload": "C3: 1024x1024x16 disk r=1 um with a 150 nm-radius hole (Ms=0 outside), 2 nm cells, "
+                        "FP32-mixed DP45 max_error 1e-5, alpha 0.1, B=(0,30,0) mT, seed 44",
+            "cells": n, "active_cells": active, "accepted_steps": steps, "warmup_steps": warm,
+            "attempts_in_profiled_window": attempts, "rejected_in_profiled_window": attempts - steps,
+            "ms_per_accepted_step": ms / steps, "value": v_all, "unit": "cell-updates/s",
+            "active_cell_updates_per_s": active * steps / (ms * 1e-3),
+            "mean_dt_s": mean_dt, "sim_time_in_window_s": float(np.sum(dts)),
+            "extrapolated_s_to_5ns_at_this_dt": 5e-9 / mean_dt * ms * 1e-3 / steps,
+            "model_bytes_per_cell_update": model,
+            "model_frac": model * v_all / 1e9 / peak, "peak_gbs": peak, "peak_kind": f"of {peak_kind}",
+            "kernels": kern, "create_s": t_create,
+            "note": "the window starts from random m0, where dt is smallest; the 5 ns figure is an upper bound"}
+
+
+def c5_adjoint_sample(steps=2000):
+    """C5 on this GPU: 256 x 256 x 1 film of 4 x 4 x 3 nm cells, per-cell Ms
+    ~ U[6e5, 1e6] (seed 46), A 1.3e-11, alpha 0.05, B(t) = (20 sin(2 pi 5 GHz t),
+    0, 5) mT, Heun dt 1e-13 x 2000, loss = sum of m_x over the central 64 x 64.
+    Per precision, CUDA events on the library's stream around: the 2000 forward
+    steps alone; the forward with sqrt(N) device checkpoints; the backward pass
+    (segment replays from the checkpoints, then the adjoint steps)."""
+    import torch
+    from fullmag_b200 import native_fdm as nf
+    nx = ny = 256
+    rng = np.random.default_rng(46)
+    ms_map = rng.uniform(6e5, 1e6, nx * ny)
+    m0 = np.tile([0.0, 1.0, 0.0], nx * ny)
+    sel = np.zeros((ny, nx), bool)
+    sel[96:160, 96:160] = True
+    g = np.zeros((nx * ny, 3))
+    g[sel.reshape(-1), 0] = 1.0
+    out = {"workload": "C5: 256x256x1, 4x4x3 nm, Ms map U[6e5,1e6], B(t)=(20 sin(2pi 5GHz t),0,5) mT, "
+                       "Heun dt 1e-13 x 2000, loss = sum m_x over the central 64x64",
+           "steps": steps, "checkpoints": int(np.ceil(np.sqrt(steps)))}
+    for prec, tag in ((nf.PRECISION_DOUBLE, "fp64"), (nf.PRECISION_SINGLE, "fp32")):
+        plan = nf.FdmPlan(cells=(nx, ny, 1), cell_size=(4e-9, 4e-9, 3e-9), initial_magnetization=m0,
+                          exchange_stiffness=1.3e-11, damping=0.05, gyromagnetic_ratio=2.211e5,
+                          precision=prec, external_field=(0.0, 0.0, 5e-3 / MU0), ms_map=ms_map,
+                          ac_field=(20e-3 / MU0, 0.0, 0.0), ac_frequency_hz=5e9, demag_source=nf.DEMAG_NEWELL)
+        be = nf.NativeFdmBackend(plan)
+        stream = torch.cuda.ExternalStream(be.stream())
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        be.step_n(1e-13, 5)  # warm-up
+        be.upload_m(m0)
+        ev[0].record(stream)
+        be.step_n(1e-13, steps)
+        ev[1].record(stream)
+        be.upload_m(m0)
+        ev[2].record(stream)
+        be.adjoint_forward(1e-13, steps)
+        ev[3].record(stream)
+        grads = be.adjoint_backward(g.reshape(-1))
+        ev[4].record(stream)
+        ev[4].synchronize()
+        fwd, fwd_ck, bwd = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]), ev[3].elapsed_time(ev[4])
+        out[tag] = {"forward_ms": fwd, "forward_with_checkpoints_ms": fwd_ck, "backward_ms": bwd,
+                    "backward_over_forward": bwd / fwd, "checkpoint_overhead": fwd_ck / fwd - 1.0,
+                    "dl_dms_abs_max": float(np.abs(grads["dl_dms"]).max()),
+                    "dl_dh_ext": [float(v) for v in grads["dl_dh_ext"]]}
+        be.close()
+    return out
+
+
 def c4_problems(count=256, seed=45):
     """Config C4: 256 problems, nx ~ U{32..256}, ny ~ U{32..128}, nz ~ U{1..4},
     isotropic cells ~ U[2, 4] nm, Ms ~ U[6e5, 1.2e6] A/m, A ~ U[1e-11, 2e-11] J/m,
@@ -417,11 +565,41 @@ def c4_problems(count=256, seed=45):
     return out
 
 
-def batch_ensemble_sample(steps=300):
+def _pow2_at_least(v):
+    p = 1
+    while p < v:
+        p *= 2
+    return p
+
+
+def batch_kind_bytes(probs, s=4):
+    """Algorithmic bytes per Heun step of each batched kernel kind (x fwd, y fwd,
+    z, y inv, x inv, stage; both evaluations of a step), summed over the
+    problems with the batch's padding (every axis to a power of two >= 2n,
+    in-plane axes >= 16)."""
+    tot = [0.0] * 6
+    cs = 2 * s
+    for p in probs:
+        nx, ny, nz = p["cells"]
+        n = nx * ny * nz
+        Lx, Ly, Lz = max(16, _pow2_at_least(2 * nx)), max(16, _pow2_at_least(2 * ny)), _pow2_at_least(2 * nz)
+        nkx = Lx // 2 + 1
+        s1 = 3 * nz * nkx * ny * cs
+        s2 = 3 * nz * nkx * Ly * cs
+        octant = 6 * (Lz // 2 + 1) * nkx * (Ly // 2 + 1) * s
+        per_eval = [3 * n * s + s1, s1 + s2, 2 * s2 + octant, s2 + s1, s1 + 3 * n * s]
+        for k in range(5):
+            tot[k] += 2 * per_eval[k]
+        tot[5] += (12 + 15) * n * s  # RHS (+ predictor) and corrector
+    return tot
+
+
+def batch_ensemble_sample(steps=1000):
     """C4 on this GPU: FP32-mixed Heun dt 5e-14 through fullmag_fdm_batch_*
     (one persistent launch per stage, one CUDA graph per step); 10 warm-up steps
-    (autotuner + graph capture), then `steps` steps timed on the host clock
-    around the synchronous step_n call."""
+    (autotuner + graph capture), then `steps` steps timed with CUDA events on the
+    batch's stream, then one step with its launches timed by kind."""
+    import torch
     from fullmag_b200 import native_fdm as nf
     probs = c4_problems()
     cells = int(sum(p["cells"][0] * p["cells"][1] * p["cells"][2] for p in probs))
@@ -429,15 +607,34 @@ def batch_ensemble_sample(steps=300):
     b = nf.NativeFdmBatch(probs, nf.PRECISION_SINGLE)
     t_create = time.time() - t0
     b.step_n(5e-14, 10)
-    t0 = time.perf_counter()
+    stream = torch.cuda.ExternalStream(b.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
     b.step_n(5e-14, steps)
-    el = time.perf_counter() - t0
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    kinds = b.profile_step(5e-14)
     tuning = b.tuning()
     b.close()
+    names = ["x_fwd", "y_fwd", "z_conv", "y_inv", "x_inv", "stage"]
+    kb = batch_kind_bytes(probs)
+    peak, peak_kind = hbm_peak()
+    per_kind = {nm: {"ms_per_step": round(kinds[i], 5), "gbs": round(kb[i] / (kinds[i] * 1e-3) / 1e9, 1)}
+                for i, nm in enumerate(names)}
+    dom = max(range(6), key=lambda i: kinds[i])
+    step_bytes = sum(kb)
     return {"workload": "C4: 256 problems, grids U{32..256} x U{32..128} x U{1..4}, FP32-mixed Heun dt 5e-14",
-            "problems": len(probs), "cells": cells, "steps": steps, "value": cells * steps / el,
-            "unit": "cell-updates/s", "ms_per_step": el / steps * 1e3, "create_s": t_create,
-            "autotuned_grid": tuning, "timing": "host clock around the synchronous step_n"}
+            "problems": len(probs), "cells": cells, "steps": steps, "value": cells * steps / (ms * 1e-3),
+            "unit": "cell-updates/s", "ms_per_step": ms / steps, "create_s": t_create,
+            "kernels": per_kind,
+            "roofline": {"kernel": names[dom], "achieved": kb[dom] / (kinds[dom] * 1e-3) / 1e9, "peak": peak,
+                         "frac": kb[dom] / (kinds[dom] * 1e-3) / 1e9 / peak, "unit": "GB/s",
+                         "peak_kind": f"of {peak_kind}"},
+            "step_bytes": step_bytes, "step_frac": step_bytes / (ms / steps * 1e-3) / 1e9 / peak,
+            "autotuned_grid": tuning,
+            "timing": "CUDA events on the batch stream around step_n (graph replays); per-kind split from "
+                      "one step with the launches issued one by one"}
 
 
 def cpu_baseline_sample():

@@ -24,6 +24,8 @@
 #include "demag.cuh"
 #include "demag_reg.cuh"
 #include "demag_yz.hpp"
+#include "demag_row.hpp"
+#include "stage_vec.hpp"
 #include "demag_yzy.hpp"
 #include "newell_host.hpp"
 #include "stages.cuh"
@@ -293,6 +295,14 @@ struct Impl {
 
     static bool demag_reg(Backend &b, const void *m, void *hd, bool unit = false) {
         DemagArgs<T> a = demag_args(b, m, hd, unit);
+        x_fwd_reg(b, a);
+        if (!mid_reg(b, a)) return false;
+        x_inv_reg(b, a);
+        return check_launch(b, "demag (register FFT)");
+    }
+
+    // x forward: Ms m -> S1
+    static void x_fwd_reg(Backend &b, const DemagArgs<T> &a) {
         const int RB = 2 * b.lines_x;
         dim3 gx((b.ny + RB - 1) / RB, b.nz, 3);
         with_split(b.Lx, [&](auto l1, auto l2) {
@@ -305,6 +315,10 @@ struct Impl {
                     k_xf_r<T, L1, L2><<<gx, b.thr_x, b.rsm_x, b.stream>>>(a);
             }
         });
+    }
+
+    // the y (thin film) or y / z passes: S1 -> S1
+    static bool mid_reg(Backend &b, const DemagArgs<T> &a) {
         if (b.thin) {
             with_split(b.Ly, [&](auto l1, auto l2) {
                 constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
@@ -359,6 +373,13 @@ struct Impl {
                 }
             });
         }
+        return true;
+    }
+
+    // x inverse: S1 -> H_d
+    static void x_inv_reg(Backend &b, const DemagArgs<T> &a) {
+        const int RB = 2 * b.lines_x;
+        dim3 gx((b.ny + RB - 1) / RB, b.nz, 3);
         with_split(b.Lx, [&](auto l1, auto l2) {
             constexpr int L1 = decltype(l1)::value, L2 = decltype(l2)::value;
             if constexpr (!(sizeof(T) == 8 && L1 > 32)) {
@@ -369,11 +390,22 @@ struct Impl {
                     k_xi_r<T, L1, L2, xi_gather<T>(), false><<<gx, b.thr_x, b.rsm_xi, b.stream>>>(a);
             }
         });
-        return check_launch(b, "demag (register FFT)");
     }
 
     // the ring-fed stage kernels' shared memory (above 48 KB for FP64)
     static bool configure_stage(Backend &b) {
+        // FP32-mixed: 16-byte cell groups with FP32 stencil and RHS when rows are
+        // whole groups and the material has at most a mask and an Ms map
+        // (FULLMAG_FDM_STAGE=ring or plain keeps the one-value-per-load kernels of
+        // a uniform material, =cell the general one).  FP64 keeps those: measured
+        // at 512 x 512 x 8 the FP64 group kernels took 84.5 / 74.2 us (RHS /
+        // corrector) against the ring's 70.0 / 60.0 us.
+        const bool rows16 = sizeof(T) == 4 && b.nx % (16 / (int)sizeof(T)) == 0;
+        const bool simple = !b.has_regions && !b.boundary_tier;
+        const bool keep = env_is("FULLMAG_FDM_STAGE", "ring") || env_is("FULLMAG_FDM_STAGE", "plain") ||
+                          env_is("FULLMAG_FDM_STAGE", "cell");
+        b.stage_vec = rows16 && simple && !keep && 3ULL * (unsigned long long)b.n < (1ULL << 32);
+        b.stage_vec_mk = b.stage_vec && (b.has_mask || b.has_ms_map);
         if (!b.stage_plain) return true;
         b.stage_ring = !env_is("FULLMAG_FDM_STAGE", "plain");
         if (!b.stage_ring) return true;
@@ -392,7 +424,7 @@ struct Impl {
         if (!upload_tw64(b)) return false;
         if (!b.force_stockham && configure_reg(b)) {
             b.use_reg = true;
-            return true;
+            return row_configure<T>(b);
         }
         b.use_reg = false;
         b.zdirect = false;
@@ -440,6 +472,8 @@ struct Impl {
     // unit: the source is m itself on active cells (no Ms), for the adjoint.
     static bool demag(Backend &b, const void *m, void *hd, bool unit = false) {
         if (!b.enable_demag) return true;
+        b.s1_state = 0;  // S1 now holds this evaluation's convolved spectrum
+        if (hd == b.hd) b.hd_stale = (m != b.m) || unit;
         if (!(b.use_reg ? demag_reg(b, m, hd, unit) : demag_stockham(b, m, hd, unit))) return false;
         if (b.corr_targets) {
             {
@@ -534,6 +568,12 @@ struct Impl {
     // general one (mask, Ms map, region LUT) otherwise.
     template <int MODE>
     static void launch_stage(Backend &b, const StageArgs<T> &s) {
+        if constexpr (sizeof(T) == 4) {
+            if (b.stage_vec) {
+                stage_vec_launch(b, s, MODE);
+                return;
+            }
+        }
         if (b.stage_plain) {
             const dim3 g((b.nx + 31) / 32, (b.ny + kStagePlainBY - 1) / kStagePlainBY,
                          (b.nz + b.stage_zb - 1) / b.stage_zb);
@@ -596,7 +636,14 @@ struct Impl {
         a.out = (T *)out;
         {
             ProfScope p(b, "stage_combine");
-            k_combine<T><<<grid_cells(b), 256, 0, b.stream>>>(a);
+            bool done = false;
+            if constexpr (sizeof(T) == 4) {
+                if (b.stage_vec && b.n % 4 == 0) {
+                    combine_vec_launch(b, a);  // 16-byte groups of cells, the group kernels' renormalisation
+                    done = true;
+                }
+            }
+            if (!done) k_combine<T><<<grid_cells(b), 256, 0, b.stream>>>(a);
         }
         return check_launch(b, "combine");
     }
@@ -627,8 +674,86 @@ struct Impl {
         return true;
     }
 
+    // One launch of the fused row pass (x inverse, stage, x forward of the new
+    // state) on S1, which holds the convolved spectrum of s.m.
+    static bool row_pass(Backend &b, int mode, const StageArgs<T> &s) {
+        const DemagArgs<T> a = demag_args(b, s.m, nullptr);
+        ProfScope p(b, mode == MODE_EVAL ? "row_eval" : mode == MODE_HEUN_CORR ? "row_heun_corr" : "row_x_fwd");
+        return row_launch(b, a, s, mode);
+    }
+
+    // S1 = X(Ms m) of state m by the row pass's own x forward (phase 4 alone)
+    static bool row_x_fwd(Backend &b, const void *m) {
+        StageArgs<T> s = stage_args(b, m, b.time);
+        return row_pass(b, MODE_ROW_XFWD, s);
+    }
+
+    // k1 = RHS(m) and the predictor normalize(m + k1 dt) into mstage by the row
+    // pass, the arithmetic of every later step, leaving S1 = X(Ms m_p).
+    static bool rows_k1(Backend &b, double dt) {
+        const DemagArgs<T> a = demag_args(b, b.m, nullptr);
+        if (!row_x_fwd(b, b.m) || !mid_reg(b, a)) return false;
+        StageArgs<T> s = stage_args(b, b.m, b.time);
+        s.kout = (T *)b.k[0];
+        s.pred_out = (T *)b.mstage;
+        s.pred_dt = dt;
+        s.counter = b.counter;
+        s.out = b.d_out;
+        if (!row_pass(b, MODE_EVAL, s)) return false;
+        b.k1_valid = b.pred_valid = true;
+        b.pred_dt = dt;
+        b.s1_state = 1;
+        return true;
+    }
+
+    // Heun with the fused row pass: per field evaluation the y / z passes and
+    // one k_row launch.  S1 carries the x transform of the predictor from one
+    // step's last launch to the next step; H_d is never written (hd_stale).
+    static bool heun_rows(Backend &b, double dt, fullmag_fdm_step_stats *st, bool readback) {
+        // k1 and the predictor come from the row pass itself, so a run gives the
+        // same bits whether it starts here or continues (checkpoint replays)
+        if (!(b.k1_valid && b.pred_valid && b.pred_dt == dt) && !rows_k1(b, dt)) return false;
+        DemagArgs<T> a = demag_args(b, b.mstage, nullptr);
+        if (b.s1_state != 1 && !row_x_fwd(b, b.mstage)) return false;
+        if (!mid_reg(b, a)) return false;
+        // corrector at m_p: m <- normalize(m0 + (k1 + k2) dt/2), S1 = X(Ms m)
+        StageArgs<T> s = stage_args(b, b.mstage, b.time + dt);
+        s.kout = nullptr;
+        s.m0 = (T *)b.m;
+        s.k1 = (const T *)b.k[0];
+        s.half_dt = 0.5 * dt;
+        if (!row_pass(b, MODE_HEUN_CORR, s)) return false;
+        b.s1_state = 0;
+        b.pred_valid = false;
+        if (!mid_reg(b, a)) return false;
+        // RHS at the new state (the next k1), diagnostics, the next predictor
+        StageArgs<T> e = stage_args(b, b.m, b.time + dt);
+        e.kout = (T *)b.k[0];
+        e.pred_out = (T *)b.mstage;
+        e.pred_dt = dt;
+        e.partials = b.partials;
+        e.counter = b.counter;
+        e.out = b.d_out;
+        if (!row_pass(b, MODE_EVAL, e)) return false;
+        b.s1_state = 1;
+        b.pred_valid = true;
+        b.pred_dt = dt;
+        b.time += dt;
+        b.step_count += 1;
+        b.k1_valid = true;
+        b.obs_valid = false;
+        b.hd_stale = true;
+        if (readback) {
+            if (!read_stats(b)) return false;
+            fill_stats(b, dt, st);
+            st->suggested_next_dt = 0.0;
+        }
+        return true;
+    }
+
     // One Heun step (lib.rs:1217-1249) with the cached k1.
     static bool heun(Backend &b, double dt, fullmag_fdm_step_stats *st, bool readback) {
+        if (b.use_row) return heun_rows(b, dt, st, readback);
         if (!ensure_k1(b)) return false;
         // predictor m_p = normalize(m + k1 dt); the previous step's RHS kernel
         // already wrote it when this dt equals the previous one
@@ -714,6 +839,7 @@ struct Impl {
             const double err = std::sqrt(b.h_out[Q_ERR2]);
             if (err <= b.max_error || dt <= b.dt_min) {
                 std::swap(b.m, b.mstage);
+                b.hd_stale = false;  // the last evaluation was at the accepted state
                 std::swap(k[0], k[6]);  // FSAL: k7 is the next step's k1
                 b.time += dt;
                 b.step_count += 1;
@@ -800,6 +926,7 @@ struct Impl {
             const double err = std::sqrt(b.h_out[Q_ERR2]);
             if (err <= b.max_error || dt <= b.dt_min) {
                 std::swap(b.m, b.mstage);
+                b.hd_stale = false;  // the last evaluation was at the accepted state
                 std::swap(k[0], k[3]);
                 b.time += dt;
                 b.step_count += 1;
@@ -1014,18 +1141,26 @@ struct Impl {
         return cuda_ok(b, cudaStreamSynchronize(b.stream), "adjoint sync");
     }
 
+    // With the fused row pass k1 is left to the next step, which computes it
+    // with the row pass's own arithmetic.
     static bool refresh(Backend &b) {
         if (!demag(b, b.m, b.hd)) return false;
-        if (!eval(b, b.m, b.time, b.k[0], false, true)) return false;
-        b.k1_valid = true;
+        if (!eval(b, b.m, b.time, b.use_row ? nullptr : b.k[0], false, true)) return false;
+        b.k1_valid = !b.use_row;
         b.obs_valid = true;
         return cuda_ok(b, cudaStreamSynchronize(b.stream), "refresh");
     }
 
+    // H_d(m) into hd when the fused Heun steps left it stale.
+    static bool ensure_hd(Backend &b) {
+        return !b.hd_stale || demag(b, b.m, b.hd);
+    }
+
     static bool ensure_obs(Backend &b) {
         if (b.obs_valid) return true;
-        // hd holds H_d(m) after a step; recompute H_ex / H_eff (and k1, unchanged)
-        if (!eval(b, b.m, b.time, b.k[0], false, true)) return false;
+        if (!ensure_hd(b)) return false;
+        // H_ex / H_eff (and k1, unchanged; the row pass keeps its own k1)
+        if (!eval(b, b.m, b.time, b.use_row ? nullptr : b.k[0], false, true)) return false;
         b.obs_valid = true;
         return true;
     }
@@ -1159,7 +1294,10 @@ bool backend_alloc(Backend &b) {
         while (zb > 1 && blocks(zb) < 148LL * 8) zb = (zb + 1) / 2;
         b.stage_zb = zb;
         const long long general = (long long)((b.nx + 31) / 32) * ((b.ny + 3) / 4) * ((b.nz + 1) / 2);
-        b.red_blocks = (int)std::max(general, blocks(zb));  // partials of either stage grid
+        const long long rows = (long long)((b.ny + 1) / 2) * b.nz;  // the row pass with 2-row slabs
+        const dim3 gv = stage_vec_grid(b, (int)b.scalar, false);      // 16-byte-group stage kernels (largest grid)
+        const long long vgrid = (long long)gv.x * gv.y * gv.z;
+        b.red_blocks = (int)std::max(std::max(general, blocks(zb)), std::max(rows, vgrid));  // partials of any stage grid
     }
     items.push_back({(void **)&b.partials, (size_t)NQ * b.red_blocks * 8});
     items.push_back({(void **)&b.counter, 64});
@@ -1235,6 +1373,7 @@ static bool upload_m_impl(Backend &b, const TI *host, uint64_t len) {
     b.k1_valid = false;
     b.pred_valid = false;
     b.obs_valid = false;
+    b.s1_state = 0;
     return cuda_ok(b, cudaStreamSynchronize(b.stream), "upload sync");
 }
 
@@ -1302,7 +1441,9 @@ static const void *observable_ptr(Backend &b, fullmag_fdm_observable obs, bool &
     ok = true;
     switch (obs) {
         case FULLMAG_FDM_OBSERVABLE_M: return b.m;
-        case FULLMAG_FDM_OBSERVABLE_H_DEMAG: return b.hd;
+        case FULLMAG_FDM_OBSERVABLE_H_DEMAG:
+            ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::ensure_hd(b) : Impl<float>::ensure_hd(b);
+            return b.hd;
         case FULLMAG_FDM_OBSERVABLE_H_EX:
         case FULLMAG_FDM_OBSERVABLE_H_EFF:
             ok = b.precision == FULLMAG_FDM_PRECISION_DOUBLE ? Impl<double>::ensure_obs(b) : Impl<float>::ensure_obs(b);

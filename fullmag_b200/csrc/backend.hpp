@@ -98,6 +98,8 @@ struct Backend {
     int grid_xpipe = 0, groups_x = 0;
     bool stage_plain = false;     // uniform material: z-marching stage kernel
     bool stage_ring = false;      // ... fed by the cp.async plane ring (FULLMAG_FDM_STAGE=plain: register prefetch)
+    bool stage_vec = false;       // stage kernels on 16-byte cell groups (stage_vec.cuh; FULLMAG_FDM_STAGE=ring/plain/cell: off)
+    bool stage_vec_mk = false;    // ... in the form with a mask and / or an Ms map
     int stage_zb = 1;             // z planes per thread of that kernel
     bool use_yz = false;          // fused y-z cluster pass (3-D, register FFT)
     bool want_yz = false;         // FULLMAG_FDM_YZ=fused selects it (default: three y/z kernels)
@@ -112,6 +114,12 @@ struct Backend {
     int yzy_P = 0;                // its cluster size (CTAs per plane)
     int grid_zd = 0;              // its persistent grid (resident blocks x SMs)
     size_t rsm_zd = 0;
+    // fused x inverse / stage / x forward row pass (Heun, uniform material)
+    bool use_row = false;
+    int row_rb = 0;               // rows per slab
+    size_t rsm_row = 0;
+    int s1_state = 0;             // S1 holds: 0 nothing usable, 1 the x transform of Ms m_stage (the predictor)
+    bool hd_stale = false;        // hd does not hold H_d(m) (fused Heun steps never write it)
 
     // ---- reductions ----
     int red_blocks = 0;

@@ -47,6 +47,22 @@ int pow2_at_least(int v) {
     return p;
 }
 
+// Padded in-plane length >= v, at least 16: in FP32 the smallest power of two
+// or 3 * 2^k in 96..768 (lengths fft4step takes with a radix-3 first level), in
+// FP64 a power of two (its batched FFT kernels already use all 255 registers; a
+// radix-3 level would spill more).  FULLMAG_FDM_BATCH_PAD=pow2 keeps powers of
+// two in FP32 too.  Measured on the 256-problem C4 draw (FP32, one process):
+// 4.98 ms per step with powers of two, 4.44 ms with 3 * 2^k from 192 and 4.08 ms
+// (another run) from 96.
+int batch_length(int v, bool dbl) {
+    int L = std::max(16, pow2_at_least(v));
+    const char *e = std::getenv("FULLMAG_FDM_BATCH_PAD");
+    if (dbl || (e && std::strcmp(e, "pow2") == 0)) return L;
+    for (int c : {96, 192, 384, 768})
+        if (c >= v && c < L) L = c;
+    return L;
+}
+
 constexpr int l2_of(int L) { return l2_for(L); }
 
 // kernel kinds tuned and launched per step
@@ -111,8 +127,8 @@ struct BatchImpl {
             if (!d.initial_magnetization_xyz) { B.last_error = "problem " + std::to_string(i) + ": initial_magnetization_xyz is null"; return false; }
             p.n = (long long)d.nx * d.ny * d.nz;
             // in-plane lengths of at least 16 (the smallest the batched x / y kernels take)
-            p.Lx = std::max(16, pow2_at_least(2 * (int)d.nx));
-            p.Ly = std::max(16, pow2_at_least(2 * (int)d.ny));
+            p.Lx = batch_length(2 * (int)d.nx, sizeof(T) == 8);
+            p.Ly = batch_length(2 * (int)d.ny, sizeof(T) == 8);
             p.Lz = pow2_at_least(2 * (int)d.nz);
             if (p.Lx > 1024 || p.Ly > 1024 || p.Lz > 16) {
                 B.last_error = "problem " + std::to_string(i) + ": grid too large for the batch (nx, ny <= 512, nz <= 8)";
@@ -412,6 +428,50 @@ struct BatchImpl {
         return batch_ok(B, cudaStreamSynchronize(B.stream), "batch step sync");
     }
 
+    // One step with every launch issued directly and timed by kind.
+    bool profile_step(fullmag_fdm_batch &B, double dt, float *ms) {
+        if (dt != args_dt) {
+            if (!upload_args(B, dt)) return false;
+            if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+            if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+            k1_valid = false;
+        }
+        if (!tuned && !tune(B)) return false;
+        if (!k1_valid) {
+            demag(B.stream, false);
+            launch(B.stream, KSTAGE, false, grid[KSTAGE]);
+            if (!batch_ok(B, cudaGetLastError(), "initial RHS")) return false;
+            k1_valid = true;
+        }
+        const int kinds[5] = {KX_FWD, KY_FWD, KZ, KY_INV, KX_INV};
+        std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev;
+        auto timed = [&](int kind, bool staged) {
+            cudaEvent_t e0, e1;
+            cudaEventCreate(&e0);
+            cudaEventCreate(&e1);
+            cudaEventRecord(e0, B.stream);
+            launch(B.stream, kind, staged, grid[kind]);
+            cudaEventRecord(e1, B.stream);
+            ev.push_back({kind, {e0, e1}});
+        };
+        for (bool staged : {true, false}) {
+            for (int k : kinds) timed(k, staged);
+            timed(KSTAGE, staged);
+        }
+        bool ok = batch_ok(B, cudaGetLastError(), "profiled step") && batch_ok(B, cudaStreamSynchronize(B.stream), "profiled step sync");
+        for (int k = 0; k < NKINDS; ++k) ms[k] = 0.f;
+        for (auto &e : ev) {
+            float t = 0.f;
+            if (ok) cudaEventElapsedTime(&t, e.second.first, e.second.second);
+            ms[e.first] += t;
+            cudaEventDestroy(e.second.first);
+            cudaEventDestroy(e.second.second);
+        }
+        time += dt;
+        steps += 1;
+        return ok;
+    }
+
     bool copy_m(fullmag_fdm_batch &B, uint32_t index, double *out) {
         const Prob &p = probs[index];
         std::vector<T> h(3 * (size_t)p.n);
@@ -433,8 +493,16 @@ bool batch_upload_tw64(fullmag_fdm_batch &B) {
         d[k] = make_double2(std::cos(a), -std::sin(a));
         f[k] = make_float2((float)d[k].x, (float)d[k].y);
     }
+    double2 d3[192];
+    float2 f3[192];
+    host_tw192(d3, f3);
+    // legacy-stream uploads from pageable memory, then a device synchronisation:
+    // the batch's stream is non-blocking
     return batch_ok(B, cudaMemcpyToSymbol(c_tw64d, d, sizeof(d)), "twiddle64 d (batch)") &&
-           batch_ok(B, cudaMemcpyToSymbol(c_tw64f, f, sizeof(f)), "twiddle64 f (batch)");
+           batch_ok(B, cudaMemcpyToSymbol(c_tw64f, f, sizeof(f)), "twiddle64 f (batch)") &&
+           batch_ok(B, cudaMemcpyToSymbol(c_tw192d, d3, sizeof(d3)), "twiddle192 d (batch)") &&
+           batch_ok(B, cudaMemcpyToSymbol(c_tw192f, f3, sizeof(f3)), "twiddle192 f (batch)") &&
+           batch_ok(B, cudaDeviceSynchronize(), "twiddle (batch) sync");
 }
 
 template <typename T>
@@ -519,6 +587,26 @@ int fullmag_fdm_batch_tuning(const fullmag_fdm_batch *B, int32_t *grid_sizes, ui
                                                                : ((BatchImpl<float> *)B->impl)->grid;
     for (int k = 0; k < fm::NKINDS; ++k) grid_sizes[k] = g[k];
     return FULLMAG_FDM_OK;
+}
+
+int fullmag_fdm_batch_get_stream(const fullmag_fdm_batch *B, void **stream_out) {
+    if (!B || !stream_out) return FULLMAG_FDM_ERR_INVALID;
+    *stream_out = (void *)B->stream;
+    return FULLMAG_FDM_OK;
+}
+
+int fullmag_fdm_batch_profile_step(fullmag_fdm_batch *B, double dt, float *ms_per_kind, uint32_t len) {
+    if (!B || !ms_per_kind || len < fm::NKINDS) return FULLMAG_FDM_ERR_INVALID;
+    if (!B->impl || !B->last_error.empty()) {
+        if (B->last_error.empty()) B->last_error = "batch was not created successfully";
+        return FULLMAG_FDM_ERR_INVALID;
+    }
+    if (!(dt > 0.0) || !std::isfinite(dt)) { B->last_error = "dt must be positive and finite"; return FULLMAG_FDM_ERR_INVALID; }
+    if (!fm::batch_ok(*B, cudaSetDevice(B->device), "cudaSetDevice")) return FULLMAG_FDM_ERR_CUDA;
+    const bool ok = B->precision == FULLMAG_FDM_PRECISION_DOUBLE
+                        ? ((BatchImpl<double> *)B->impl)->profile_step(*B, dt, ms_per_kind)
+                        : ((BatchImpl<float> *)B->impl)->profile_step(*B, dt, ms_per_kind);
+    return ok ? FULLMAG_FDM_OK : FULLMAG_FDM_ERR_CUDA;
 }
 
 const char *fullmag_fdm_batch_last_error(const fullmag_fdm_batch *B) {

@@ -16,7 +16,8 @@
 namespace fm {
 
 // x passes: item (p, bx, z, c); 256 threads, lines_x = 256 / L2 per problem;
-// Lx in 16..1024 (batch.cu pads every in-plane axis to at least 16)
+// Lx a power of two in 16..1024, or in FP32 3 * 2^k in 96..768 (batch.cu pads
+// every in-plane axis to at least 16)
 template <typename T, bool INV>
 __global__ void __launch_bounds__(256) k_batch_x(const DemagArgs<T> *__restrict__ A, const int4 *__restrict__ work,
                                                  int nwork) {
@@ -32,9 +33,13 @@ __global__ void __launch_bounds__(256) k_batch_x(const DemagArgs<T> *__restrict_
             case 16: FM_X(16, 1)
             case 32: FM_X(32, 1)
             case 64: FM_X(8, 8)
+            case 96: if constexpr (sizeof(T) == 4) { FM_X(24, 4) } break;
             case 128: FM_X(16, 8)
+            case 192: if constexpr (sizeof(T) == 4) { FM_X(24, 8) } break;
             case 256: FM_X(16, 16)
+            case 384: if constexpr (sizeof(T) == 4) { FM_X(48, 8) } break;
             case 512: FM_X(32, 16)
+            case 768: if constexpr (sizeof(T) == 4) { FM_X(48, 16) } break;
             case 1024: FM_X(32, 32)
 #undef FM_X
             default: break;
@@ -59,9 +64,13 @@ __global__ void __launch_bounds__(256) k_batch_y(const DemagArgs<T> *__restrict_
             case 16: FM_Y(16, 1)
             case 32: FM_Y(32, 1)
             case 64: FM_Y(8, 8)
+            case 96: if constexpr (sizeof(T) == 4) { FM_Y(24, 4) } break;
             case 128: FM_Y(16, 8)
+            case 192: if constexpr (sizeof(T) == 4) { FM_Y(24, 8) } break;
             case 256: FM_Y(16, 16)
+            case 384: if constexpr (sizeof(T) == 4) { FM_Y(48, 8) } break;
             case 512: FM_Y(32, 16)
+            case 768: if constexpr (sizeof(T) == 4) { FM_Y(48, 16) } break;
             case 1024: FM_Y(32, 32)
 #undef FM_Y
             default: break;

@@ -70,7 +70,41 @@ __device__ __forceinline__ void xf_body(const DemagArgs<T> &a, int bx, int z, in
         return v;
     };
     auto out = [&](int k, C v) { line[k] = v; };
-    fft4step<L1, L2, false, false, true, true>(t, tw, line, in, out);
+    if (!PAD && a.mask && !a.ms_map && !a.vf && !a.unit_source && nx % 16 == 0) {
+        // masked rows: each line group first copies its two rows of m and of the
+        // mask into its own region with 16-byte loads (many in flight), then the
+        // transform reads them from there; per-element global loads under the
+        // mask test stalled on memory latency (issue active 9 % at 2048-point lines)
+        // 8-byte chunks: a line region starts on 8 bytes (its stride is odd in FP32)
+        T *rm = reinterpret_cast<T *>(line);                                 // m rows: reals [0, 2 nx)
+        unsigned char *rk = reinterpret_cast<unsigned char *>(rm + 2 * nx);  // mask rows: bytes [0, 2 nx)
+        constexpr int PT = 8 / (int)sizeof(T);
+        const int cm = 2 * nx / PT, ck = 2 * nx / 8;
+        for (int u = t; u < cm + ck; u += L2) {
+            if (u < cm) {
+                const int e = u * PT, r = e >= nx, x = e - r * nx, yy = r ? yb : ya;
+                uint2 v = make_uint2(0u, 0u);
+                if (yy < ny) v = *reinterpret_cast<const uint2 *>(mc + (r ? rowb : rowa) + x);
+                *reinterpret_cast<uint2 *>(rm + e) = v;
+            } else {
+                const int e = (u - cm) * 8, r = e >= nx, x = e - r * nx, yy = r ? yb : ya;
+                uint2 v = make_uint2(0u, 0u);
+                if (yy < ny) v = *reinterpret_cast<const uint2 *>(a.mask + (r ? rowb : rowa) + x);
+                *reinterpret_cast<uint2 *>(rk + e) = v;
+            }
+        }
+        __syncthreads();
+        // M = Ms m on active cells, the product as demag_source forms it
+        auto in_s = [&](int j) -> C {
+            C v = mk<T>(0, 0);
+            if (rk[j]) v.x = (T)((double)rm[j] * a.ms);
+            if (rk[nx + j]) v.y = (T)((double)rm[nx + j] * a.ms);
+            return v;
+        };
+        fft4step<L1, L2, false, true, true, true>(t, tw, line, in_s, out);
+    } else {
+        fft4step<L1, L2, false, false, true, true>(t, tw, line, in, out);
+    }
     __syncthreads();
     const int nkx = a.nkx;
     C *s1row = a.s1 + ((long long)c * a.nz + z) * nkx * ny;

@@ -25,15 +25,24 @@
 namespace fm {
 
 // exp(-2 pi i k / 64), k < 64, filled per device by the host (upload_tw64).
-// Defined here: one translation unit (backend.cu) includes this header.
+// Every translation unit that includes this header holds its own copy and
+// fills it.
 __constant__ double2 c_tw64d[64];
 __constant__ float2 c_tw64f[64];
+// exp(-2 pi i k / 192), k < 192, for the radix-3 stage of fft_reg3 (filled by
+// the units whose kernels use lengths 3 * 2^k: upload_tw192)
+__constant__ double2 c_tw192d[192];
+__constant__ float2 c_tw192f[192];
 
 template <typename C> __device__ __forceinline__ C tw64(int k);
 template <> __device__ __forceinline__ double2 tw64<double2>(int k) { return c_tw64d[k]; }
 template <> __device__ __forceinline__ float2 tw64<float2>(int k) { return c_tw64f[k]; }
+template <typename C> __device__ __forceinline__ C tw192(int k);
+template <> __device__ __forceinline__ double2 tw192<double2>(int k) { return c_tw192d[k]; }
+template <> __device__ __forceinline__ float2 tw192<float2>(int k) { return c_tw192f[k]; }
 
 template <int N> __host__ __device__ constexpr int ilog2() { return N <= 1 ? 0 : 1 + ilog2<N / 2>(); }
+template <int N> __host__ __device__ constexpr bool is_pow2c() { return N >= 1 && (N & (N - 1)) == 0; }
 
 template <int N> __host__ __device__ constexpr int brev(int k) {
     int r = 0;
@@ -72,6 +81,58 @@ __device__ __forceinline__ void fft_reg(C (&v)[N]) {
     }
 }
 
+// N = 3 M (M a power of two <= 16) held in one thread's registers: a radix-3
+// decimation-in-frequency stage over x[j], x[j + M], x[j + 2 M] (twiddles
+// W_N^{j r} from the W_192 table, compile-time indices), then fft_reg<M> on each
+// third.  Output of element k = 3 k' + r at v[r M + brev<M>(k')] (perm_any).
+template <int N, bool INV, typename C>
+__device__ __forceinline__ void fft_reg3(C (&v)[N]) {
+    constexpr int M = N / 3;
+    static_assert(N == 3 * M && is_pow2c<M>() && M <= 16, "fft_reg3 size");
+    using T = decltype(v[0].x);
+    const T h = T(0.8660254037844386);  // sin(pi / 3)
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+        const C a = v[j], b = v[j + M], c = v[j + 2 * M];
+        const C sm = cadd(b, c), df = csub(b, c);
+        C t = a;
+        t.x = a.x - T(0.5) * sm.x;
+        t.y = a.y - T(0.5) * sm.y;
+        C u = rot_i<INV>(df);  // -i (b - c) forward, +i inverse
+        u.x *= h;
+        u.y *= h;
+        v[j] = cadd(a, sm);
+        C x1 = cadd(t, u), x2 = csub(t, u);
+        if (j != 0) {
+            const C w1 = tw192<C>(j * (64 / M)), w2 = tw192<C>(2 * j * (64 / M));
+            x1 = INV ? cmulc(x1, w1) : cmul(x1, w1);
+            x2 = INV ? cmulc(x2, w2) : cmul(x2, w2);
+        }
+        v[j + M] = x1;
+        v[j + 2 * M] = x2;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        C g[M];
+#pragma unroll
+        for (int j = 0; j < M; ++j) g[j] = v[r * M + j];
+        fft_reg<M, INV>(g);
+#pragma unroll
+        for (int j = 0; j < M; ++j) v[r * M + j] = g[j];
+    }
+}
+
+// a power of two (fft_reg) or three times one (fft_reg3), and where output k sits
+template <int N, bool INV, typename C>
+__device__ __forceinline__ void fft_any(C (&v)[N]) {
+    if constexpr (is_pow2c<N>()) fft_reg<N, INV>(v);
+    else fft_reg3<N, INV>(v);
+}
+template <int N> __host__ __device__ constexpr int perm_any(int k) {
+    if constexpr (is_pow2c<N>()) return brev<N>(k);
+    else return (k % 3) * (N / 3) + brev<N / 3>(k / 3);
+}
+
 // Inverse (or forward) FFT of bit-reversed-ordered input, natural-order
 // output: radix-2 decimation in time, the transpose of fft_reg's network.
 // Lets a caller go forward with fft_reg, work on the spectrum where it lies
@@ -94,10 +155,12 @@ __device__ __forceinline__ void fft_reg_dit(C (&v)[N]) {
     }
 }
 
-// Sizes of the two levels for a line length L (power of two, 2..4096):
-// L1 values per thread in registers, L2 threads per line.
+// Sizes of the two levels for a line length L (a power of two 2..4096, or
+// 3 * 2^k: 48, 96, 192, 384, 768): L1 values per thread in registers (L1 = L /
+// L2, a multiple of L2), L2 threads per line.
 __host__ __device__ constexpr int l2_for(int L) {
-    return L <= 32 ? 1 : L == 64 ? 8 : L == 128 ? 8 : L == 256 ? 16 : L == 512 ? 16
+    return L <= 32 || L == 48 ? 1 : L == 96 ? 4 : L == 192 || L == 384 ? 8 : L == 768 ? 16
+         : L == 64 ? 8 : L == 128 ? 8 : L == 256 ? 16 : L == 512 ? 16
          : L == 1024 ? 32 : L == 2048 ? 32 : 64;
 }
 
@@ -130,6 +193,15 @@ inline std::vector<cx<T>> host_tw4(int L) {
     return t;
 }
 
+// Host: the W_192 table of fft_reg3 (double and float copies).
+inline void host_tw192(double2 (&d)[192], float2 (&f)[192]) {
+    for (int k = 0; k < 192; ++k) {
+        const double a = 2.0 * kPi * (double)k / 192.0;
+        d[k] = make_double2(std::cos(a), -std::sin(a));
+        f[k] = make_float2((float)d[k].x, (float)d[k].y);
+    }
+}
+
 // One line, L2 threads; t = thread index within the line group.
 //   in(j)        -> C   for j = t + L2 * i
 //   out(k, v)           for k = k1 + L1 * k2 (this thread's k1 = t + L2 * r)
@@ -151,16 +223,16 @@ __device__ __forceinline__ void fft4step(int t, const C *__restrict__ tw, C *til
         if (HALF_IN && i >= L1 / 2) { v[i].x = 0; v[i].y = 0; }
         else v[i] = in(t + L2 * i);
     }
-    fft_reg<L1, INV>(v);
+    fft_any<L1, INV>(v);
     if constexpr (L2 == 1) {
         if (ALIAS_OUT) __syncthreads();
 #pragma unroll
-        for (int k1 = 0; k1 < L1; ++k1) out(k1, v[brev<L1>(k1)]);
+        for (int k1 = 0; k1 < L1; ++k1) out(k1, v[perm_any<L1>(k1)]);
     } else {
         if (ALIAS_IN) __syncthreads();
 #pragma unroll
         for (int k1 = 0; k1 < L1; ++k1) {
-            C x = v[brev<L1>(k1)];
+            C x = v[perm_any<L1>(k1)];
             if (k1 != 0 && t != 0) {
                 const C w = tw[k1 * L2 + t];
                 x = INV ? cmulc(x, w) : cmul(x, w);

@@ -109,9 +109,11 @@ __device__ __forceinline__ bool st_active(const StageArgs<T> &a, long long i, do
 template <typename T>
 __device__ __forceinline__ void store_predictor(const StageArgs<T> &a, size_t i, size_t n, const double (&c)[3],
                                                 double r0, double r1, double r2) {
-    const double v0 = c[0] + (double)(T)r0 * a.pred_dt;
-    const double v1 = c[1] + (double)(T)r1 * a.pred_dt;
-    const double v2 = c[2] + (double)(T)r2 * a.pred_dt;
+    // one explicit fused multiply-add, as every predictor site of the library
+    // (the stage kernels and combine form 0), so that all give the same bits
+    const double v0 = __fma_rn((double)(T)r0, a.pred_dt, c[0]);
+    const double v1 = __fma_rn((double)(T)r1, a.pred_dt, c[1]);
+    const double v2 = __fma_rn((double)(T)r2, a.pred_dt, c[2]);
     const double n2 = v0 * v0 + v1 * v1 + v2 * v2;
     double inv;
     if (sizeof(T) == 8) {
@@ -796,7 +798,9 @@ __device__ __forceinline__ void combine_cell(const CombineArgs<T> &a, long long 
                            ((double)a.k[3][o] * a.c[3] + (double)a.k[4][o] * a.c[4])) * a.dt;
                     break;
             }
-            v[comp] = (double)a.m0[o] + inc;
+            // form 0 is the predictor: one explicit fused multiply-add like the
+            // stage kernels' predictor (store_predictor), the same bits
+            v[comp] = a.form == 0 ? __fma_rn((double)a.k[0][o], a.c[0], (double)a.m0[o]) : (double)a.m0[o] + inc;
         }
         const double n2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
         double inv;

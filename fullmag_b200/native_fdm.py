@@ -127,6 +127,7 @@ EXT_FUNCTIONS = (
     "fullmag_fdm_adjoint_forward", "fullmag_fdm_adjoint_backward",
     "fullmag_fdm_batch_create", "fullmag_fdm_batch_step_n", "fullmag_fdm_batch_copy_m",
     "fullmag_fdm_batch_tuning", "fullmag_fdm_batch_last_error", "fullmag_fdm_batch_destroy",
+    "fullmag_fdm_batch_get_stream", "fullmag_fdm_batch_profile_step",
 )
 
 class BatchProblem(C.Structure):
@@ -204,6 +205,8 @@ def load_library(build_if_missing: bool = True):
     L.fullmag_fdm_batch_last_error.restype = C.c_char_p
     L.fullmag_fdm_batch_last_error.argtypes = [vp]
     L.fullmag_fdm_batch_destroy.argtypes = [vp]
+    L.fullmag_fdm_batch_get_stream.argtypes = [vp, C.POINTER(C.c_void_p)]
+    L.fullmag_fdm_batch_profile_step.argtypes = [vp, C.c_double, C.POINTER(C.c_float), C.c_uint32]
     L.fullmag_fdm_batch_destroy.restype = None
     _lib = L
     return L
@@ -604,6 +607,17 @@ class NativeFdmBatch:
         self._check(self._lib.fullmag_fdm_batch_copy_m(self._h, index, out.ctypes.data_as(_dp), out.size),
                     "batch_copy_m")
         return out
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        self._check(self._lib.fullmag_fdm_batch_get_stream(self._h, C.byref(p)), "batch_get_stream")
+        return int(p.value or 0)
+
+    def profile_step(self, dt: float) -> list:
+        """One step, launches timed by kind (ms): x fwd, y fwd, z, y inv, x inv, stage, predictor."""
+        ms = (C.c_float * 7)()
+        self._check(self._lib.fullmag_fdm_batch_profile_step(self._h, dt, ms, 7), "batch_profile_step")
+        return [float(v) for v in ms]
 
     def tuning(self):
         g = (C.c_int32 * 7)()

@@ -82,7 +82,10 @@ int fullmag_fdm_adjoint_backward(fullmag_fdm_backend *handle, const double *dl_d
  * alpha, gamma, static field and m0) stepped together with Heun: every stage
  * of a step is one persistent launch over all problems, and a step is one
  * CUDA graph.  Grids up to 512 x 512 x 8 cells; the demag spectra are the
- * library's FP64 Newell tensor (no mask, regions or boundary tiers).  On the
+ * library's FP64 Newell tensor (no mask, regions or boundary tiers), for each
+ * problem's padding: x and y to the smallest power of two >= 2n, or in FP32
+ * the smallest power of two or 3 * 2^k (96, 192, 384, 768) >= 2n; z to a power
+ * of two >= 2 nz.  On the
  * first fullmag_fdm_batch_step_n call an autotuner picks each kernel's
  * persistent grid size; fullmag_fdm_batch_tuning reports the picks (7 values:
  * x forward, y forward, z convolution, y inverse, x inverse, stage, predictor).
@@ -108,6 +111,16 @@ int fullmag_fdm_batch_copy_m(fullmag_fdm_batch *batch, uint32_t index, double *o
 int fullmag_fdm_batch_tuning(const fullmag_fdm_batch *batch, int32_t *grid_sizes, uint32_t len);
 const char *fullmag_fdm_batch_last_error(const fullmag_fdm_batch *batch);
 void fullmag_fdm_batch_destroy(fullmag_fdm_batch *batch);
+/* The CUDA stream (cudaStream_t) the batch's kernels and graphs run on, for
+ * timing with events. */
+int fullmag_fdm_batch_get_stream(const fullmag_fdm_batch *batch, void **stream_out);
+/* One Heun step of the whole batch with its launches issued one by one (not as
+ * the graph) and CUDA events around each: ms_per_kind[k] is the device time of
+ * kernel kind k during that step, for the 7 kinds of fullmag_fdm_batch_tuning
+ * (each demag kind runs twice per step, the stage kernel twice, the predictor
+ * kernel not at all).  The batch advances by that step. */
+int fullmag_fdm_batch_profile_step(fullmag_fdm_batch *batch, double dt_seconds, float *ms_per_kind,
+                                   uint32_t len);
 
 /* Per-kernel device timing with CUDA events on the library's stream. */
 int fullmag_fdm_backend_set_profiling(fullmag_fdm_backend *handle, int enable);

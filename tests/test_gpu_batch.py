@@ -3,8 +3,10 @@ uneven grids and materials, stepped together with one persistent launch per
 stage and one CUDA graph per step, against the FP64 oracle run alone on that
 problem.  Tolerances as for single problems: FP64 max|dm| <= 1e-10 after 10
 Heun steps (inside the predictability horizon of random m0), FP32-mixed 1e-5.
-The batch pads each axis to a power of two >= 2n, the oracle to 2n: the
-fields agree in exact arithmetic (kernel offsets |r| <= n - 1 only)."""
+The batch pads each in-plane axis to the smallest power of two or (FP32) 3 * 2^k
+(96, 192, 384, 768) >= 2n and z to a power of two, the oracle to 2n: the fields
+agree in exact arithmetic (kernel offsets |r| <= n - 1 only).  The shapes cover
+padded lengths 16, 32, 64, 96, 128, 192, 256 and 384."""
 import numpy as np
 import pytest
 
@@ -14,7 +16,8 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 MU0 = 4e-7 * np.pi
-SHAPES = [(37, 23, 1), (64, 32, 2), (45, 61, 3), (32, 32, 4), (100, 50, 1), (16, 128, 2), (7, 9, 3)]
+SHAPES = [(37, 23, 1), (64, 32, 2), (45, 61, 3), (32, 32, 4), (100, 50, 1), (16, 128, 2), (7, 9, 3),
+          (90, 70, 2), (170, 40, 1)]
 
 
 def _problems(seed=45):

@@ -464,12 +464,12 @@ def test_heun_dt_change_and_upload_recompute_the_predictor():
     assert max_abs(be.copy_m(), sim.m) <= 1e-10
 
 
-# The uniform-material stage kernels come in two forms that share the per-cell
-# arithmetic: loads prefetched one plane ahead into registers
+# The one-value-per-load uniform-material stage kernels come in two forms that
+# share the per-cell arithmetic: loads prefetched one plane ahead into registers
 # (FULLMAG_FDM_STAGE=plain), or copied several planes ahead into a per-thread
-# shared-memory ring (default).  They must agree bit for bit: the state, every
-# field, and every step statistic, also for DP45's last stage (error norm) and
-# on grids whose edges cut warps and blocks.
+# shared-memory ring (FULLMAG_FDM_STAGE=ring).  They must agree bit for bit: the
+# state, every field, and every step statistic, also for DP45's last stage
+# (error norm) and on grids whose edges cut warps and blocks.
 @pytest.mark.parametrize("prec", [nf.PRECISION_DOUBLE, nf.PRECISION_SINGLE])
 @pytest.mark.parametrize("integrator", [nf.HEUN, nf.DP45])
 def test_stage_ring_matches_register_prefetch(monkeypatch, prec, integrator):
@@ -477,7 +477,7 @@ def test_stage_ring_matches_register_prefetch(monkeypatch, prec, integrator):
               precision=prec, integrator=integrator, seed=21)
     if integrator == nf.DP45:
         kw["adaptive"] = (1e-6, 1e-16, 1e-12, 0.8)
-    monkeypatch.delenv("FULLMAG_FDM_STAGE", raising=False)
+    monkeypatch.setenv("FULLMAG_FDM_STAGE", "ring")
     ring, _, _ = make_pair(**kw)
     monkeypatch.setenv("FULLMAG_FDM_STAGE", "plain")
     plain, _, _ = make_pair(**kw)
@@ -491,6 +491,52 @@ def test_stage_ring_matches_register_prefetch(monkeypatch, prec, integrator):
     plain.refresh_observables()
     for o in (nf.OBS_H_EX, nf.OBS_H_DEMAG, nf.OBS_H_EFF):
         assert np.array_equal(ring.copy_field(o), plain.copy_field(o)), o
+
+
+# The FP32-mixed stage kernels work on 16-byte groups of cells (k_stage_vec)
+# with the stencil and RHS in FP32: against the FP64 oracle at the FP32-mixed
+# bound (1e-5), and against the FP32-mixed one-value-per-load kernels with the
+# RHS in FP64 (FULLMAG_FDM_STAGE=ring / cell) at the same bound, with and
+# without a mask and an Ms map, Heun and DP45 (error norm), on grids whose edges
+# cut warps and blocks.  Inactive cells stay exactly zero.
+@pytest.mark.parametrize("integrator", [nf.HEUN, nf.DP45])
+@pytest.mark.parametrize("cells,form", [((40, 25, 5), None), ((120, 9, 3), None), ((8, 4, 1), None),
+                                        ((48, 40, 3), "mask"), ((48, 40, 3), "ms_map"), ((48, 40, 3), "both")])
+def test_stage_vec_fp32_matches_oracle_and_scalar_kernels(monkeypatch, integrator, cells, form):
+    nx, ny, nz = cells
+    n = nx * ny * nz
+    rng = np.random.default_rng(8)
+    mask = _disk_mask(nx, ny, nz, 38e-9, 9e-9, 2e-9) if form in ("mask", "both") else None
+    ms_map = rng.uniform(6e5, 1e6, n) if form in ("ms_map", "both") else None
+    if ms_map is not None:
+        ms_map[rng.integers(0, n, 40)] = 0.0  # inactive through Ms as well
+    kw = dict(cells=cells, cell_size=(2e-9, 2e-9, 2.5e-9), alpha=0.2, h_ext=(1e4, -2e4, 5e3),
+              integrator=integrator, seed=21, mask=mask, ms_map=ms_map, precision=nf.PRECISION_SINGLE)
+    if integrator == nf.DP45:
+        kw["adaptive"] = (1e-6, 1e-16, 1e-12, 0.8)
+    monkeypatch.delenv("FULLMAG_FDM_STAGE", raising=False)
+    vec, sim, _ = make_pair(**kw)
+    monkeypatch.setenv("FULLMAG_FDM_STAGE", "cell" if form else "ring")
+    ref, _, _ = make_pair(**kw)
+    dt = 2e-14
+    for k in range(8):
+        sa, sb, r = vec.step(dt), ref.step(dt), sim.step(dt)
+        if integrator == nf.DP45:
+            dt = sa["suggested_next_dt"]
+    assert abs(sa["total_energy_joules"] - r["e_total"]) <= 1e-4 * abs(r["e_total"])
+    m = vec.copy_m()
+    d_oracle, d_ref = max_abs(m, sim.m), max_abs(m, ref.copy_m())
+    print(cells, form, integrator, f"FP32-mixed vec vs oracle {d_oracle:.2e}, vs scalar kernels {d_ref:.2e}")
+    assert d_oracle <= 1e-5 and d_ref <= 1e-5
+    inactive = np.zeros(n, bool)
+    if mask is not None:
+        inactive |= mask == 0
+    if ms_map is not None:
+        inactive |= ms_map <= 0.0
+    assert np.all(m.reshape(-1, 3)[inactive] == 0.0)
+    obs = sim.observe()
+    for o, key in ((nf.OBS_H_EX, "h_ex"), (nf.OBS_H_DEMAG, "h_demag"), (nf.OBS_H_EFF, "h_eff")):
+        assert max_abs(vec.copy_field(o), obs[key]) <= 1e-4 * np.abs(obs[key]).max(), o
 
 
 # Grids with the direct z table and Ly = 2 ny in 256..1024 run the y forward
