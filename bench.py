@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-c5", action="store_true", help="skip the adjoint (C5) timing")
     ap.add_argument("--kernels-only", action="store_true",
                     help="FP32-mixed warm-up + K timed steps only (for profiler runs)")
+    ap.add_argument("--c3-band", type=int, default=0, metavar="NY",
+                    help="profiler run: the C3 geometry cut to 1024 x NY x 16, FP32-mixed DP45, "
+                         "K accepted steps after W, per-kernel times of the last")
     return ap.parse_args()
 
 
@@ -696,8 +699,39 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def c3_band_run(ny, steps, warm):
+    """The C3 geometry cut to a 1024 x ny x 16 band (ny <= 1024; the disk
+    centred in the band), FP32-mixed DP45 as in c3_masked_dp45_sample: `warm`
+    accepted steps, then `steps` more with per-kernel CUDA events; prints one
+    JSON line.  A case for profiler captures that holds a few GB at most."""
+    import torch  # noqa: F401  (CUDA context through the library)
+    from fullmag_b200 import native_fdm as nf
+    nx, nz, d = 1024, 16, 2e-9
+    n = nx * ny * nz
+    mask = c3_mask(nx, ny, nz, d)
+    plan = nf.FdmPlan(cells=(nx, ny, nz), cell_size=(d, d, d), initial_magnetization=nf.random_unit_vectors(44, n),
+                      saturation_magnetisation=8e5, exchange_stiffness=1.3e-11, damping=0.1,
+                      gyromagnetic_ratio=2.211e5, precision=nf.PRECISION_SINGLE, integrator=nf.DP45,
+                      external_field=(0.0, 30e-3 / MU0, 0.0), active_mask=mask,
+                      adaptive=(1e-5, 1e-18, 1e-10, 0.8), demag_source=nf.DEMAG_NEWELL)
+    be = nf.NativeFdmBackend(plan)
+    dt = 1e-13
+    for _ in range(warm):
+        dt = be.step(dt)["suggested_next_dt"]
+    be.set_profiling(True)
+    for _ in range(steps):
+        dt = be.step(dt)["suggested_next_dt"]
+    prof = be.profile()
+    be.close()
+    print(json.dumps({"mode": "c3-band", "cells": [nx, ny, nz], "steps": steps,
+                      "kernels_ms_per_launch": {k: v[0] / v[1] for k, v in sorted(prof.items())}}))
+
+
 def main():
     args = parse()
+    if args.c3_band:
+        c3_band_run(args.c3_band, args.steps, args.warmup)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

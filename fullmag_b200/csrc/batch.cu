@@ -88,7 +88,11 @@ struct BatchImpl {
     int *d_zb = nullptr;
     int4 *dW[NKINDS] = {};
     int nW[NKINDS] = {};
-    size_t smem_x = 0, smem_y = 0;
+    size_t smem_x = 0, smem_y = 0;   // for 256-thread x / y blocks (the larger tile)
+    // tile shape of the x and y passes, chosen by the autotuner: threads per block
+    // (128 or 256), so a block holds tpb / L2 lines of each problem
+    int tpb_x = 256, tpb_y = 256;
+    int capW[NKINDS] = {};           // work-list capacity (the 128-thread lists are the longest)
     int grid[NKINDS] = {};
     bool tuned = false, k1_valid = false;
     double args_dt = -1.0;
@@ -155,24 +159,12 @@ struct BatchImpl {
                 }
             }
         }
-        // work lists
+        // work lists (x and y: for 128-thread blocks, the longest; rebuilt per tile shape)
         std::vector<int4> W[NKINDS];
+        xy_lists(128, 128, W);
         for (uint32_t i = 0; i < count; ++i) {
             const Prob &p = probs[i];
-            const int nx = p.d.nx, ny = p.d.ny, nz = p.d.nz;
-            const int RB = 2 * (256 / l2_of(p.Lx));
-            for (int c = 0; c < 3; ++c)
-                for (int z = 0; z < nz; ++z)
-                    for (int bx = 0; bx < (ny + RB - 1) / RB; ++bx) {
-                        W[KX_FWD].push_back(make_int4((int)i, bx, z, c));
-                        W[KX_INV].push_back(make_int4((int)i, bx, z, c));
-                    }
-            const int ly = 256 / l2_of(p.Ly);
-            const long long lines = 3LL * nz * p.nkx;
-            for (long long bx = 0; bx < (lines + ly - 1) / ly; ++bx) {
-                W[KY_FWD].push_back(make_int4((int)i, (int)bx, 0, 0));
-                W[KY_INV].push_back(make_int4((int)i, (int)bx, 0, 0));
-            }
+            const int nx = p.d.nx, ny = p.d.ny;
             const int P = p.Lz > 8 ? 2 : 1;
             const long long tasks = (long long)p.nkx * p.Ly * P;
             for (long long ch = 0; ch < (tasks + 127) / 128; ++ch) W[KZ].push_back(make_int4((int)i, (int)ch, 0, 0));
@@ -187,7 +179,7 @@ struct BatchImpl {
         size_t o_C = take(count * sizeof(CombineArgs<T>)), o_zb = take(count * sizeof(int));
         size_t o_W[NKINDS];
         for (int k = 0; k < NKINDS; ++k) {
-            nW[k] = (int)W[k].size();
+            nW[k] = capW[k] = (int)W[k].size();
             o_W[k] = take(W[k].size() * sizeof(int4));
         }
         (void)off_tables;
@@ -252,7 +244,46 @@ struct BatchImpl {
                   batch_ok(B, cudaFuncSetAttribute(k_batch_y<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y), "attr y") &&
                   batch_ok(B, cudaFuncSetAttribute(k_batch_y<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y), "attr y");
         if (!ok) return false;
-        return upload_args(B, 1e-13);
+        return set_tiles(B, 256, 256) && upload_args(B, 1e-13);
+    }
+
+    // x / y work lists for tx- and ty-thread blocks: x item (problem, row block of
+    // 2 tx / L2 rows, z, component), y item (problem, block of ty / L2 lines)
+    void xy_lists(int tx, int ty, std::vector<int4> (&W)[NKINDS]) const {
+        for (int k : {KX_FWD, KX_INV, KY_FWD, KY_INV}) W[k].clear();
+        for (size_t i = 0; i < probs.size(); ++i) {
+            const Prob &p = probs[i];
+            const int ny = p.d.ny, nz = p.d.nz;
+            const int RB = 2 * std::max(1, tx / l2_of(p.Lx));
+            for (int c = 0; c < 3; ++c)
+                for (int z = 0; z < nz; ++z)
+                    for (int bx = 0; bx < (ny + RB - 1) / RB; ++bx) {
+                        W[KX_FWD].push_back(make_int4((int)i, bx, z, c));
+                        W[KX_INV].push_back(make_int4((int)i, bx, z, c));
+                    }
+            const int ly = std::max(1, ty / l2_of(p.Ly));
+            const long long lines = 3LL * nz * p.nkx;
+            for (long long bx = 0; bx < (lines + ly - 1) / ly; ++bx) {
+                W[KY_FWD].push_back(make_int4((int)i, (int)bx, 0, 0));
+                W[KY_INV].push_back(make_int4((int)i, (int)bx, 0, 0));
+            }
+        }
+    }
+
+    // Switch the x / y tile shape: work lists and the lines per block in the
+    // argument tables (uploaded with the next upload_args).
+    bool set_tiles(fullmag_fdm_batch &B, int tx, int ty) {
+        std::vector<int4> W[NKINDS];
+        xy_lists(tx, ty, W);
+        for (int k : {KX_FWD, KX_INV, KY_FWD, KY_INV}) {
+            if ((int)W[k].size() > capW[k]) { B.last_error = "batch work list overflow"; return false; }
+            nW[k] = (int)W[k].size();
+            if (nW[k] && !batch_ok(B, cudaMemcpy(dW[k], W[k].data(), W[k].size() * sizeof(int4), cudaMemcpyHostToDevice), "upload work list"))
+                return false;
+        }
+        tpb_x = tx;
+        tpb_y = ty;
+        return true;
     }
 
     const C *tw(int L) {
@@ -291,8 +322,8 @@ struct BatchImpl {
             a.ms = d.saturation_magnetisation;
             a.hd = hd;
             a.norm = 1.0 / ((double)p.Lx * (double)p.Ly * (double)p.Lz);
-            a.lines_x = 256 / l2_of(p.Lx);
-            a.lines_y = 256 / l2_of(p.Ly);
+            a.lines_x = std::max(1, tpb_x / l2_of(p.Lx));
+            a.lines_y = std::max(1, tpb_y / l2_of(p.Ly));
             a.m = m;
             hA_m[i] = a;
             a.m = ms;
@@ -339,11 +370,11 @@ struct BatchImpl {
     void launch(cudaStream_t st, int kind, bool staged, int G) {
         const DemagArgs<T> *A = staged ? dA_s : dA_m;
         switch (kind) {
-            case KX_FWD: k_batch_x<T, false><<<g(kind, G), 256, smem_x, st>>>(A, dW[kind], nW[kind]); break;
-            case KY_FWD: k_batch_y<T, false><<<g(kind, G), 256, smem_y, st>>>(A, dW[kind], nW[kind]); break;
+            case KX_FWD: k_batch_x<T, false><<<g(kind, G), tpb_x, smem_x * tpb_x / 256, st>>>(A, dW[kind], nW[kind]); break;
+            case KY_FWD: k_batch_y<T, false><<<g(kind, G), tpb_y, smem_y * tpb_y / 256, st>>>(A, dW[kind], nW[kind]); break;
             case KZ: k_batch_z<T><<<g(kind, G), 128, 0, st>>>(A, dW[kind], nW[kind]); break;
-            case KY_INV: k_batch_y<T, true><<<g(kind, G), 256, smem_y, st>>>(A, dW[kind], nW[kind]); break;
-            case KX_INV: k_batch_x<T, true><<<g(kind, G), 256, smem_x, st>>>(A, dW[kind], nW[kind]); break;
+            case KY_INV: k_batch_y<T, true><<<g(kind, G), tpb_y, smem_y * tpb_y / 256, st>>>(A, dW[kind], nW[kind]); break;
+            case KX_INV: k_batch_x<T, true><<<g(kind, G), tpb_x, smem_x * tpb_x / 256, st>>>(A, dW[kind], nW[kind]); break;
             case KSTAGE:
                 if (staged)
                     k_batch_stage<T, MODE_HEUN_CORR><<<g(kind, G), dim3(32, kStagePlainBY), 0, st>>>(dS_corr, d_zb, dW[kind], nW[kind]);
@@ -359,17 +390,19 @@ struct BatchImpl {
         for (int k : kinds) launch(st, k, staged, grid[k]);
     }
 
-    // Autotuner: persistent grid size per kernel from {1, 2, 4, 8, 16} blocks
-    // per SM, by CUDA-event time of two launches each (after one warm-up).
+    // Autotuner: for the x and y passes the tile shape (128- or 256-thread blocks,
+    // so tpb / L2 lines of a problem per block) together with the persistent grid
+    // size; for the other kernels the grid size; grid sizes from {1, 2, 4, 8, 16}
+    // blocks per SM; by CUDA-event time of two launches each (after one warm-up).
     // The stage kernel is tuned in its RHS form, which writes only k1.
     bool tune(fullmag_fdm_batch &B) {
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B.device);
         cudaEvent_t e0, e1;
         if (!batch_ok(B, cudaEventCreate(&e0), "event") || !batch_ok(B, cudaEventCreate(&e1), "event")) return false;
-        for (int k = 0; k < NKINDS; ++k) {
-            float best = 1e30f;
-            int best_g = sms;
+        auto tune_kind = [&](int k, float &best, int &best_g) -> bool {
+            best = 1e30f;
+            best_g = sms;
             const int pers[5] = {1, 2, 4, 8, 16};
             for (int per : pers) {
                 const int G = sms * per;
@@ -384,7 +417,26 @@ struct BatchImpl {
                 if (ms < best) { best = ms; best_g = G; }
                 if (G >= nW[k]) break;
             }
-            grid[k] = best_g;
+            return true;
+        };
+        int tx = 256, ty = 256, gx[2] = {sms, sms}, gy[2] = {sms, sms};
+        float bx = 1e30f, by = 1e30f;
+        for (int t : {256, 128}) {
+            if (!set_tiles(B, t, t) || !upload_args(B, args_dt)) return false;
+            float f[4];
+            int g4[4];
+            const int kinds[4] = {KX_FWD, KX_INV, KY_FWD, KY_INV};
+            for (int i = 0; i < 4; ++i)
+                if (!tune_kind(kinds[i], f[i], g4[i])) return false;
+            if (f[0] + f[1] < bx) { bx = f[0] + f[1]; tx = t; gx[0] = g4[0]; gx[1] = g4[1]; }
+            if (f[2] + f[3] < by) { by = f[2] + f[3]; ty = t; gy[0] = g4[2]; gy[1] = g4[3]; }
+        }
+        if (!set_tiles(B, tx, ty) || !upload_args(B, args_dt)) return false;
+        grid[KX_FWD] = gx[0]; grid[KX_INV] = gx[1];
+        grid[KY_FWD] = gy[0]; grid[KY_INV] = gy[1];
+        for (int k : {KZ, KSTAGE, KCOMB}) {
+            float f;
+            if (!tune_kind(k, f, grid[k])) return false;
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -583,9 +635,13 @@ int fullmag_fdm_batch_copy_m(fullmag_fdm_batch *B, uint32_t index, double *out_x
 
 int fullmag_fdm_batch_tuning(const fullmag_fdm_batch *B, int32_t *grid_sizes, uint32_t len) {
     if (!B || !grid_sizes || len < fm::NKINDS || !B->impl) return FULLMAG_FDM_ERR_INVALID;
-    const int *g = B->precision == FULLMAG_FDM_PRECISION_DOUBLE ? ((BatchImpl<double> *)B->impl)->grid
-                                                               : ((BatchImpl<float> *)B->impl)->grid;
+    const bool dbl = B->precision == FULLMAG_FDM_PRECISION_DOUBLE;
+    const int *g = dbl ? ((BatchImpl<double> *)B->impl)->grid : ((BatchImpl<float> *)B->impl)->grid;
     for (int k = 0; k < fm::NKINDS; ++k) grid_sizes[k] = g[k];
+    if (len >= fm::NKINDS + 2) {  // the tile shape: threads per block of the x and y passes
+        grid_sizes[fm::NKINDS] = dbl ? ((BatchImpl<double> *)B->impl)->tpb_x : ((BatchImpl<float> *)B->impl)->tpb_x;
+        grid_sizes[fm::NKINDS + 1] = dbl ? ((BatchImpl<double> *)B->impl)->tpb_y : ((BatchImpl<float> *)B->impl)->tpb_y;
+    }
     return FULLMAG_FDM_OK;
 }
 

@@ -245,6 +245,8 @@ __device__ __forceinline__ void sv_group(const StageArgs<T> &a, const PlainConst
     if ((MODE == MODE_EVAL && a.pred_out) || MODE == MODE_HEUN_CORR) {
         // the new state in FP64: predictor normalize(m + k dt), corrector
         // normalize(m0 + (k1 + k2) dt / 2)
+        // the corrector's m0 and k1 here (issued with the stencil's loads at 120
+        // registers the kernel measured 45.4 us against 41.0 at C2)
         SVec<T> m0v[3], k1v[3], nw[3];
         if (MODE == MODE_HEUN_CORR) {
 #pragma unroll

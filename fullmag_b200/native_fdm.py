@@ -620,8 +620,10 @@ class NativeFdmBatch:
         return [float(v) for v in ms]
 
     def tuning(self):
-        g = (C.c_int32 * 7)()
-        self._check(self._lib.fullmag_fdm_batch_tuning(self._h, g, 7), "batch_tuning")
+        """The autotuner's picks: 7 grid sizes (x fwd, y fwd, z, y inv, x inv,
+        stage, predictor), then the x and y passes' threads per block."""
+        g = (C.c_int32 * 9)()
+        self._check(self._lib.fullmag_fdm_batch_tuning(self._h, g, 9), "batch_tuning")
         return list(g)
 
     def close(self) -> None:

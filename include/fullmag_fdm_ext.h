@@ -87,8 +87,10 @@ int fullmag_fdm_adjoint_backward(fullmag_fdm_backend *handle, const double *dl_d
  * the smallest power of two or 3 * 2^k (96, 192, 384, 768) >= 2n; z to a power
  * of two >= 2 nz.  On the
  * first fullmag_fdm_batch_step_n call an autotuner picks each kernel's
- * persistent grid size; fullmag_fdm_batch_tuning reports the picks (7 values:
- * x forward, y forward, z convolution, y inverse, x inverse, stage, predictor).
+ * persistent grid size and the tile shape of the x and y passes (128- or
+ * 256-thread blocks); fullmag_fdm_batch_tuning reports the picks (7 grid sizes:
+ * x forward, y forward, z convolution, y inverse, x inverse, stage, predictor;
+ * with len >= 9 also the x and y passes' threads per block).
  * create returns a handle even on failure, with last_error set (NULL only when
  * the handle itself cannot be allocated). */
 typedef struct {

@@ -52,7 +52,8 @@ def test_batch_matches_oracle_per_problem(precision, tol):
         b.step_n(dt, 4)
         b.step_n(dt, n - 4)   # the graph is replayed; two calls = one trajectory
         tuning = b.tuning()
-        assert len(tuning) == 7 and all(g > 0 for g in tuning), tuning
+        assert len(tuning) == 9 and all(g > 0 for g in tuning), tuning
+        assert tuning[7] in (128, 256) and tuning[8] in (128, 256), tuning  # x / y tile shape
         for i, p in enumerate(probs):
             err = np.abs(b.copy_m(i) - _oracle(p, dt, n)).max()
             print(i, p["cells"], f"{err:.2e}")
