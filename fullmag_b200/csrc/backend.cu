@@ -27,6 +27,7 @@
 #include "demag_row.hpp"
 #include "stage_vec.hpp"
 #include "demag_yzy.hpp"
+#include "demag_zdw.hpp"
 #include "newell_host.hpp"
 #include "stages.cuh"
 #include "adjoint.cuh"
@@ -191,13 +192,15 @@ struct Impl {
 
     // Register-FFT path: power-of-two x/y lengths <= 1024 (FP64) or 4096 (FP32).
     // z: direct summation for nz <= 8 (any nz; FULLMAG_FDM_ZCONV=fft keeps the
-    // z FFT), else the register z FFT, Lz a power of two <= 16 (FP64) or 32
-    // (FP32) since a thread holds 3 z lines.
+    // z FFT) and in FP32 for nz <= 16 (k_zdw), else the register z FFT, Lz a
+    // power of two <= 16 (FP64) or 32 (FP32) since a thread holds 3 z lines.
     static bool configure_reg(Backend &b) {
         const bool dbl = sizeof(T) == 8;
         const int maxxy = dbl ? 1024 : 4096, maxz = dbl ? 16 : 32;
         if (!is_pow2(b.Lx) || !is_pow2(b.Ly) || b.Lx > maxxy || b.Ly > maxxy) return false;
-        b.zdirect = !b.thin && b.nz <= 8 && !b.want_yz && !env_is("FULLMAG_FDM_ZCONV", "fft");
+        const bool zdw = zdw_wanted(b, !dbl);
+        b.use_zdw = false;
+        b.zdirect = zdw || (!b.thin && b.nz <= 8 && !b.want_yz && !env_is("FULLMAG_FDM_ZCONV", "fft"));
         if (!b.thin && !b.zdirect && (!is_pow2(b.Lz) || b.Lz > maxz)) return false;
         const size_t sz = sizeof(C), maxs = 200 * 1024;
         const int target = 128;  // x passes: small blocks, several per SM
@@ -289,7 +292,11 @@ struct Impl {
             });
         }
         b.use_yzy = false;
-        if (ok && b.zdirect) ok &= yzy_configure<T>(b);
+        if (ok && zdw) {
+            ok &= zdw_configure(b);
+            if (ok && !b.use_zdw) return false;  // no resident block: the generic path
+        }
+        if (ok && b.zdirect && !b.use_zdw) ok &= yzy_configure<T>(b);
         return ok;
     }
 
@@ -343,7 +350,10 @@ struct Impl {
                     k_yf_r<T, L1, L2><<<gy, b.thr_y, b.rsm_y, b.stream>>>(a);
                 }
             });
-            if (b.zdirect) {
+            if (b.use_zdw) {
+                ProfScope p(b, "demag_z_direct");
+                if constexpr (sizeof(T) == 4) zdw_launch(b, a);
+            } else if (b.zdirect) {
                 ProfScope p(b, "demag_z_direct");
                 with_nz(b.nz, [&](auto nzc) {
                     constexpr int NZ = decltype(nzc)::value;
@@ -429,6 +439,7 @@ struct Impl {
         b.use_reg = false;
         b.zdirect = false;
         b.use_yzy = false;
+        b.use_zdw = false;
         if (!b.last_error.empty()) return false;
         const int budget = 100 * 1024;
         const int sz = (int)sizeof(C);

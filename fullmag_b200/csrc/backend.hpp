@@ -109,11 +109,14 @@ struct Backend {
     size_t rsm_x = 0, rsm_y = 0, rsm_yc = 0;
     size_t rsm_xi = 0;            // x inverse: line regions + twiddle table
     bool xi_pair = false;         // x inverse gathers row pairs (ny even)
-    bool zdirect = false;         // 3-D, nz <= 8: z convolution by direct summation (k_zd)
+    bool zdirect = false;         // 3-D, nz <= 8 (FP32: nz <= 16): z convolution by direct summation (k_zd, k_zdw)
     bool use_yzy = false;         // y forward + direct z + y inverse fused per kx plane (k_yzy)
     int yzy_P = 0;                // its cluster size (CTAs per plane)
     int grid_zd = 0;              // its persistent grid (resident blocks x SMs)
     size_t rsm_zd = 0;
+    bool use_zdw = false;         // FP32, 8 < nz <= 16: the direct z sum split by output half (k_zdw)
+    int grid_zdw = 0;
+    size_t rsm_zdw = 0;
     // fused x inverse / stage / x forward row pass (Heun, uniform material)
     bool use_row = false;
     int row_rb = 0;               // rows per slab

@@ -85,6 +85,17 @@ __global__ void __launch_bounds__(yzy_threads<T, L2, NZ, P>()) k_yzy(DemagArgs<T
     __syncthreads();  // fft4step reads twiddles before its first barrier
     const int kx = blockIdx.x / P, nkx = a.nkx, ny = a.ny;
     const int qg = threadIdx.x / L2, t = threadIdx.x - qg * L2;
+    {   // only the z sum reads the plane's table (6 NZ rows of KY values): bring it
+        // into L2 while the y forward FFTs run, the rows split over the cluster's CTAs
+        constexpr int LN = 128 / (int)sizeof(T);  // values per 128-byte line
+        const int KY = a.KY, nln = (KY + LN - 1) / LN;
+        const T *t0 = a.spec + (long long)kx * KY;
+        for (int i = h * BT + threadIdx.x; i < 6 * NZ * nln; i += P * BT) {
+            const int r = i / nln, j = i - r * nln;
+            const T *p = t0 + (long long)r * nkx * KY + min(j * LN, KY - 1);
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+        }
+    }
     // 1. forward y, LPP lines per pass: inputs y < ny (= L/2; the upper half is the
     // zero padding).  Every thread takes part in every pass (fft4step has barriers).
 #pragma unroll 1
