@@ -1352,9 +1352,19 @@ static bool upload_tables(Backend &b, const std::vector<double> (&spec)[6]) {
     if (b.zdirect) octant_to_z_direct(b.nkx, b.KY, b.nz, spec, zt);
     const auto &src = b.zdirect ? zt : spec;
     const size_t plane = (size_t)(b.zdirect ? b.nz : b.KZ) * b.nkx * b.KY;
-    std::vector<T> host(6 * plane);
-    for (int c = 0; c < 6; ++c)
-        for (size_t o = 0; o < plane; ++o) host[c * plane + o] = (T)src[c][o];
+    std::vector<T> host;
+    if (b.use_zdw && b.zdw_win) {
+        // rows of zdw_kyp values (16-byte windows of k_zdw), the padding zero
+        const size_t kyp = (size_t)b.zdw_kyp, rows = (size_t)b.nz * b.nkx;
+        host.assign(6 * rows * kyp, T(0));
+        for (int c = 0; c < 6; ++c)
+            for (size_t r = 0; r < rows; ++r)
+                for (int ky = 0; ky < b.KY; ++ky) host[(c * rows + r) * kyp + ky] = (T)src[c][r * b.KY + ky];
+    } else {
+        host.resize(6 * plane);
+        for (int c = 0; c < 6; ++c)
+            for (size_t o = 0; o < plane; ++o) host[c * plane + o] = (T)src[c][o];
+    }
     return cuda_ok(b, cudaMemcpy(b.spec, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice), "spectra upload");
 }
 

@@ -115,6 +115,8 @@ struct Backend {
     int grid_zd = 0;              // its persistent grid (resident blocks x SMs)
     size_t rsm_zd = 0;
     bool use_zdw = false;         // FP32, 8 < nz <= 16: the direct z sum split by output half (k_zdw)
+    bool zdw_win = false;         // ... in its window form: z table rows padded to zdw_kyp values
+    int zdw_kyp = 0;
     int grid_zdw = 0;
     size_t rsm_zdw = 0;
     // fused x inverse / stage / x forward row pass (Heun, uniform material)

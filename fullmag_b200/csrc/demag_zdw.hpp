@@ -12,7 +12,10 @@ namespace fm {
 // against k_zd); FULLMAG_FDM_ZCONV=fft keeps the z FFT.
 bool zdw_wanted(const Backend &b, bool fp32);
 // Sets b.use_zdw, b.grid_zdw and b.rsm_zdw (persistent grid: resident blocks
-// x SMs).  False only on a CUDA error that leaves the backend unusable.
+// x SMs), and b.zdw_win / b.zdw_kyp for the window form (Ly % 128 == 0; the
+// table is then uploaded with rows of zdw_kyp values; FULLMAG_FDM_ZDW=elem
+// keeps the element copies).  False only on a CUDA error that leaves the
+// backend unusable.
 bool zdw_configure(Backend &b);
 void zdw_launch(Backend &b, const DemagArgs<float> &a);
 

@@ -19,21 +19,33 @@ bool zdw_wanted(const Backend &b, bool fp32) {
 
 bool zdw_configure(Backend &b) {
     b.use_zdw = false;
+    // window form: Ly a multiple of 128 and the padded table within the octant's
+    // allocation (6 KZ nkx KY values; KY >= 3 nz is enough)
+    const int kyp = (b.KY + 3) / 4 * 4;
+    b.zdw_win = b.Ly % 128 == 0 && (long long)b.nz * kyp <= (long long)b.KZ * b.KY &&
+                !zdw_env("FULLMAG_FDM_ZDW", "elem");
+    b.zdw_kyp = b.zdw_win ? kyp : 0;
     bool ok = true;
     zdw_with_nz(b.nz, [&](auto nzc) {
         constexpr int NZ = decltype(nzc)::value;
-        constexpr size_t smem = zdw_smem<NZ>();
-        int occ = 0, sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.device);
-        ok &= cuda_ok(b, cudaFuncSetAttribute(k_zdw<NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                      "attr zdw");
-        ok &= cuda_ok(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_zdw<NZ>, kZdwThreads, smem),
-                      "occupancy zdw");
-        if (!ok || occ < 1) return;
-        const long long batches = ((long long)b.nkx * b.Ly + kZdwCols - 1) / kZdwCols;
-        b.grid_zdw = (int)std::max<long long>(1, std::min<long long>(batches, (long long)occ * sms));
-        b.rsm_zdw = smem;
-        b.use_zdw = true;
+        auto cfg = [&](auto kern, size_t smem) {
+            int occ = 0, sms = 148;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.device);
+            ok &= cuda_ok(b, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                          "attr zdw");
+            // the largest shared-memory carveout, so that two blocks fit per SM
+            ok &= cuda_ok(b, cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                  (int)cudaSharedmemCarveoutMaxShared), "carveout zdw");
+            ok &= cuda_ok(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kZdwThreads, smem),
+                          "occupancy zdw");
+            if (!ok || occ < 1) return;
+            const long long batches = ((long long)b.nkx * b.Ly + kZdwCols - 1) / kZdwCols;
+            b.grid_zdw = (int)std::max<long long>(1, std::min<long long>(batches, (long long)occ * sms));
+            b.rsm_zdw = smem;
+            b.use_zdw = true;
+        };
+        if (b.zdw_win) cfg(k_zdw<NZ, true>, zdw_smem<NZ, true>());
+        else cfg(k_zdw<NZ, false>, zdw_smem<NZ, false>());
     });
     return ok;
 }
@@ -41,7 +53,8 @@ bool zdw_configure(Backend &b) {
 void zdw_launch(Backend &b, const DemagArgs<float> &a) {
     zdw_with_nz(b.nz, [&](auto nzc) {
         constexpr int NZ = decltype(nzc)::value;
-        k_zdw<NZ><<<b.grid_zdw, kZdwThreads, b.rsm_zdw, b.stream>>>(a);
+        if (b.zdw_win) k_zdw<NZ, true><<<b.grid_zdw, kZdwThreads, b.rsm_zdw, b.stream>>>(a, b.zdw_kyp);
+        else k_zdw<NZ, false><<<b.grid_zdw, kZdwThreads, b.rsm_zdw, b.stream>>>(a, 0);
     });
 }
 
