@@ -575,22 +575,34 @@ def _pow2_at_least(v):
     return p
 
 
-def batch_kind_bytes(probs, s=4):
+def _batch_length(v, dbl=False):
+    """The batch's padded in-plane length (batch.cu batch_length): at least 16,
+    the smallest power of two >= v, or in FP32 3 * 2^k in 96..768 when shorter."""
+    L = max(16, _pow2_at_least(v))
+    if not dbl:
+        for c in (96, 192, 384, 768):
+            if v <= c < L:
+                L = c
+    return L
+
+
+def batch_kind_bytes(probs, s=4, zdirect=True):
     """Algorithmic bytes per Heun step of each batched kernel kind (x fwd, y fwd,
     z, y inv, x inv, stage; both evaluations of a step), summed over the
-    problems with the batch's padding (every axis to a power of two >= 2n,
-    in-plane axes >= 16)."""
+    problems with the batch's padding (in-plane lengths as batch_length, z to a
+    power of two >= 2 nz).  The z kind reads the direct table (nz planes per
+    component) or, with the z FFT, the octant (Lz / 2 + 1 planes)."""
     tot = [0.0] * 6
     cs = 2 * s
     for p in probs:
         nx, ny, nz = p["cells"]
         n = nx * ny * nz
-        Lx, Ly, Lz = max(16, _pow2_at_least(2 * nx)), max(16, _pow2_at_least(2 * ny)), _pow2_at_least(2 * nz)
+        Lx, Ly, Lz = _batch_length(2 * nx, s == 8), _batch_length(2 * ny, s == 8), _pow2_at_least(2 * nz)
         nkx = Lx // 2 + 1
         s1 = 3 * nz * nkx * ny * cs
         s2 = 3 * nz * nkx * Ly * cs
-        octant = 6 * (Lz // 2 + 1) * nkx * (Ly // 2 + 1) * s
-        per_eval = [3 * n * s + s1, s1 + s2, 2 * s2 + octant, s2 + s1, s1 + 3 * n * s]
+        table = 6 * (nz if zdirect else Lz // 2 + 1) * nkx * (Ly // 2 + 1) * s
+        per_eval = [3 * n * s + s1, s1 + s2, 2 * s2 + table, s2 + s1, s1 + 3 * n * s]
         for k in range(5):
             tot[k] += 2 * per_eval[k]
         tot[5] += (12 + 15) * n * s  # RHS (+ predictor) and corrector
@@ -621,7 +633,7 @@ def batch_ensemble_sample(steps=1000):
     tuning = b.tuning()
     b.close()
     names = ["x_fwd", "y_fwd", "z_conv", "y_inv", "x_inv", "stage"]
-    kb = batch_kind_bytes(probs)
+    kb = batch_kind_bytes(probs, zdirect=os.environ.get("FULLMAG_FDM_BATCH_ZCONV") != "fft")
     peak, peak_kind = hbm_peak()
     per_kind = {nm: {"ms_per_step": round(kinds[i], 5), "gbs": round(kb[i] / (kinds[i] * 1e-3) / 1e9, 1)}
                 for i, nm in enumerate(names)}

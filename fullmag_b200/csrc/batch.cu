@@ -7,7 +7,9 @@
 // length gives the reference's field, see newell_octant_spectra_padded); a
 // film (nz = 1) takes the 3-D pipeline with Lz = 2, the CPU engine's form.
 // The autotuner times each stage kernel at persistent grid sizes of 1..16
-// blocks per SM on the first call and keeps the fastest.
+// blocks per SM on the first call and keeps the fastest.  The z convolution is
+// summed directly over the unpadded z (a table of nz planes per problem, built
+// from its octant at its Lz), or by z FFTs with FULLMAG_FDM_BATCH_ZCONV=fft.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -95,6 +97,10 @@ struct BatchImpl {
     int capW[NKINDS] = {};           // work-list capacity (the 128-thread lists are the longest)
     int grid[NKINDS] = {};
     bool tuned = false, k1_valid = false;
+    // z convolution: direct sums over the unpadded z with each problem's table
+    // (octant_to_z_direct at its Lz), or FULLMAG_FDM_BATCH_ZCONV=fft: z FFTs
+    bool zdirect = true;
+    int zmax = 1;                    // the largest nz of the batch
     double args_dt = -1.0;
     double time = 0.0;
     uint64_t steps = 0;
@@ -114,6 +120,10 @@ struct BatchImpl {
 
     bool create(fullmag_fdm_batch &B, const fullmag_fdm_batch_problem *ps, uint32_t count) {
         const size_t s = sizeof(T), cs = 2 * sizeof(T);
+        {
+            const char *z = std::getenv("FULLMAG_FDM_BATCH_ZCONV");
+            zdirect = !(z && std::strcmp(z, "fft") == 0);
+        }
         size_t off = 0;
         auto take = [&](size_t bytes) {
             const size_t o = off;
@@ -130,6 +140,7 @@ struct BatchImpl {
             if (!(d.saturation_magnetisation > 0)) { B.last_error = "problem " + std::to_string(i) + ": saturation_magnetisation must be positive"; return false; }
             if (!d.initial_magnetization_xyz) { B.last_error = "problem " + std::to_string(i) + ": initial_magnetization_xyz is null"; return false; }
             p.n = (long long)d.nx * d.ny * d.nz;
+            zmax = std::max(zmax, (int)d.nz);
             // in-plane lengths of at least 16 (the smallest the batched x / y kernels take)
             p.Lx = batch_length(2 * (int)d.nx, sizeof(T) == 8);
             p.Ly = batch_length(2 * (int)d.ny, sizeof(T) == 8);
@@ -159,13 +170,15 @@ struct BatchImpl {
                 }
             }
         }
+        // FP64 sums of nz > 4 hold more registers than a thread has: z FFTs there
+        if (sizeof(T) == 8 && zmax > 4) zdirect = false;
         // work lists (x and y: for 128-thread blocks, the longest; rebuilt per tile shape)
         std::vector<int4> W[NKINDS];
         xy_lists(128, 128, W);
         for (uint32_t i = 0; i < count; ++i) {
             const Prob &p = probs[i];
             const int nx = p.d.nx, ny = p.d.ny;
-            const int P = p.Lz > 8 ? 2 : 1;
+            const int P = (!zdirect && p.Lz > 8) ? 2 : 1;
             const long long tasks = (long long)p.nkx * p.Ly * P;
             for (long long ch = 0; ch < (tasks + 127) / 128; ++ch) W[KZ].push_back(make_int4((int)i, (int)ch, 0, 0));
             for (int bz = 0; bz < 1; ++bz)
@@ -217,12 +230,16 @@ struct BatchImpl {
         for (uint32_t i = 0; i < count; ++i) {
             Prob &p = probs[i];
             const auto &d = p.d;
-            std::vector<double> spec[6];
+            std::vector<double> spec[6], zt[6];
             newell_octant_spectra_padded(d.nx, d.ny, d.nz, d.dx, d.dy, d.dz, false, p.Lx, p.Ly, p.Lz, spec);
-            const size_t plane = (size_t)p.KZ * p.nkx * p.KY;
+            // the direct table has nz planes per component (nz <= Lz / 2 < KZ: it
+            // fits the octant's allocation)
+            if (zdirect) octant_to_z_direct(p.nkx, p.KY, (int)d.nz, spec, zt, p.Lz / 2);
+            const auto &src = zdirect ? zt : spec;
+            const size_t plane = (size_t)(zdirect ? (int)d.nz : p.KZ) * p.nkx * p.KY;
             std::vector<T> host(6 * plane);
             for (int c = 0; c < 6; ++c)
-                for (size_t o = 0; o < plane; ++o) host[c * plane + o] = (T)spec[c][o];
+                for (size_t o = 0; o < plane; ++o) host[c * plane + o] = (T)src[c][o];
             if (!batch_ok(B, cudaMemcpy(base() + p.off_spec, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice), "upload spectra"))
                 return false;
             std::vector<T> m(3 * (size_t)p.n);
@@ -372,7 +389,12 @@ struct BatchImpl {
         switch (kind) {
             case KX_FWD: k_batch_x<T, false><<<g(kind, G), tpb_x, smem_x * tpb_x / 256, st>>>(A, dW[kind], nW[kind]); break;
             case KY_FWD: k_batch_y<T, false><<<g(kind, G), tpb_y, smem_y * tpb_y / 256, st>>>(A, dW[kind], nW[kind]); break;
-            case KZ: k_batch_z<T><<<g(kind, G), 128, 0, st>>>(A, dW[kind], nW[kind]); break;
+            case KZ:
+                if (zdirect && zmax <= 4) k_batch_z<T, true, 4><<<g(kind, G), 128, 0, st>>>(A, dW[kind], nW[kind]);
+                else if (zdirect) {
+                    if constexpr (sizeof(T) == 4) k_batch_z<T, true, 8><<<g(kind, G), 128, 0, st>>>(A, dW[kind], nW[kind]);
+                } else k_batch_z<T, false><<<g(kind, G), 128, 0, st>>>(A, dW[kind], nW[kind]);
+                break;
             case KY_INV: k_batch_y<T, true><<<g(kind, G), tpb_y, smem_y * tpb_y / 256, st>>>(A, dW[kind], nW[kind]); break;
             case KX_INV: k_batch_x<T, true><<<g(kind, G), tpb_x, smem_x * tpb_x / 256, st>>>(A, dW[kind], nW[kind]); break;
             case KSTAGE:

@@ -79,20 +79,95 @@ __global__ void __launch_bounds__(256) k_batch_y(const DemagArgs<T> *__restrict_
     }
 }
 
-// z convolution: item (p, chunk) of 128 column tasks; 128 threads
-template <typename T>
+// Direct z sum of one column (col = kx Ly + ky) with the table of
+// octant_to_z_direct: the arithmetic of k_zd in the same order per output,
+// inputs and table entries read straight from global memory.
+template <typename T, int NZ>
+__device__ __forceinline__ void zd_col(const DemagArgs<T> &a, int col) {
+    using C = cx<T>;
+    const int Ly = a.Ly, KY = a.KY, cols = a.nkx * Ly;
+    if (col >= cols) return;
+    const int cs = NZ * cols, dstr = a.nkx * KY, tstr = NZ * dstr;
+    const int kx = col / Ly, ky = col - kx * Ly;
+    const bool ymir = ky > Ly / 2;
+    const T sy = ymir ? T(-1) : T(1);
+    const T *tp = a.spec + (kx * KY + (ymir ? Ly - ky : ky));
+    C *base = a.s2 + col;
+    C mx[NZ], my[NZ], mz[NZ], hx[NZ], hy[NZ], hz[NZ];
+#pragma unroll
+    for (int z = 0; z < NZ; ++z) {
+        mx[z] = base[z * cols];
+        my[z] = base[cs + z * cols];
+        const C v = base[2 * cs + z * cols];
+        mz[z] = mk<T>(v.y, -v.x);  // -i Mz
+        hx[z] = mk<T>(0, 0); hy[z] = mk<T>(0, 0); hz[z] = mk<T>(0, 0);
+    }
+#pragma unroll
+    for (int d = 0; d < NZ; ++d) {
+        const T *qd = tp + d * dstr;
+        const T cxx = qd[0], cyy = qd[tstr], czz = qd[2 * tstr], cxy = qd[3 * tstr] * sy;
+        const T cxz = d > 0 ? qd[4 * tstr] : T(0), cyz = d > 0 ? qd[5 * tstr] * sy : T(0);
+#pragma unroll
+        for (int z = 0; z + d < NZ; ++z) {
+            {   // output z + d from input z (offset +d)
+                const int o = z + d;
+                zd_fma(hx[o], cxx, mx[z]); zd_fma(hx[o], cxy, my[z]); zd_fma(hx[o], cxz, mz[z]);
+                zd_fma(hy[o], cxy, mx[z]); zd_fma(hy[o], cyy, my[z]); zd_fma(hy[o], cyz, mz[z]);
+                zd_fma(hz[o], -cxz, mx[z]); zd_fma(hz[o], -cyz, my[z]); zd_fma(hz[o], czz, mz[z]);
+            }
+            if (d > 0) {  // output z from input z + d (offset -d: odd-in-z entries flip)
+                const int i = z + d;
+                zd_fma(hx[z], cxx, mx[i]); zd_fma(hx[z], cxy, my[i]); zd_fma(hx[z], -cxz, mz[i]);
+                zd_fma(hy[z], cxy, mx[i]); zd_fma(hy[z], cyy, my[i]); zd_fma(hy[z], -cyz, mz[i]);
+                zd_fma(hz[z], cxz, mx[i]); zd_fma(hz[z], cyz, my[i]); zd_fma(hz[z], czz, mz[i]);
+            }
+        }
+    }
+#pragma unroll
+    for (int z = 0; z < NZ; ++z) {
+        base[z * cols] = hx[z];
+        base[cs + z * cols] = hy[z];
+        base[2 * cs + z * cols] = mk<T>(-hz[z].y, hz[z].x);  // Hz = i Hz'
+    }
+}
+
+// z convolution: item (p, chunk) of 128 column tasks; 128 threads.  DIRECT: the
+// direct sum per column for nz <= NZMAX (the kernel's registers are those of
+// its largest case, so batches whose problems all have nz <= 4 take NZMAX = 4),
+// else the z FFT pass (zc_task; with Lz = 16 a thread pair per column)
+template <typename T, bool DIRECT, int NZMAX = 8>
 __global__ void __launch_bounds__(128) k_batch_z(const DemagArgs<T> *__restrict__ A, const int4 *__restrict__ work,
                                                  int nwork) {
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const int4 it = work[w];
         const DemagArgs<T> &a = A[it.x];
         const int tid = it.y * 128 + threadIdx.x;
-        switch (a.Lz) {
-            case 2: zc_task<T, 2, 1>(a, tid, 0); break;
-            case 4: zc_task<T, 4, 1>(a, tid, 0); break;
-            case 8: zc_task<T, 8, 1>(a, tid, 0); break;
-            case 16: zc_task<T, 16, 2>(a, tid, threadIdx.x & 1); break;
-            default: break;
+        if constexpr (DIRECT) {
+            switch (a.nz) {
+                case 1: zd_col<T, 1>(a, tid); break;
+                case 2: zd_col<T, 2>(a, tid); break;
+                case 3: zd_col<T, 3>(a, tid); break;
+                case 4: zd_col<T, 4>(a, tid); break;
+                default:
+                    if constexpr (NZMAX > 4) {
+                        switch (a.nz) {
+                            case 5: zd_col<T, 5>(a, tid); break;
+                            case 6: zd_col<T, 6>(a, tid); break;
+                            case 7: zd_col<T, 7>(a, tid); break;
+                            case 8: zd_col<T, 8>(a, tid); break;
+                            default: break;
+                        }
+                    }
+                    break;
+            }
+        } else {
+            switch (a.Lz) {
+                case 2: zc_task<T, 2, 1>(a, tid, 0); break;
+                case 4: zc_task<T, 4, 1>(a, tid, 0); break;
+                case 8: zc_task<T, 8, 1>(a, tid, 0); break;
+                case 16: zc_task<T, 16, 2>(a, tid, threadIdx.x & 1); break;
+                default: break;
+            }
         }
     }
 }

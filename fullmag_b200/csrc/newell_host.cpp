@@ -269,16 +269,17 @@ void newell_octant_spectra_padded(int nx, int ny, int nz, double dx, double dy, 
 }
 
 void octant_to_z_direct(int nkx, int KY, int nz, const std::vector<double> (&spec)[6],
-                        std::vector<double> (&out)[6]) {
+                        std::vector<double> (&out)[6], int h) {
+    if (h <= 0) h = nz;
     const size_t plane = (size_t)nkx * KY;
     const bool oddz[6] = {false, false, false, false, true, true};
-    // cos / sin (pi k d / nz) for k, d < nz
-    std::vector<double> cs((size_t)nz * nz), sn((size_t)nz * nz);
+    // cos / sin (pi k d / h) for d < nz, k < h
+    std::vector<double> cs((size_t)nz * h), sn((size_t)nz * h);
     for (int d = 0; d < nz; ++d)
-        for (int k = 0; k < nz; ++k) {
-            const double a = PI * (double)k * (double)d / (double)nz;
-            cs[d * nz + k] = std::cos(a);
-            sn[d * nz + k] = std::sin(a);
+        for (int k = 0; k < h; ++k) {
+            const double a = PI * (double)k * (double)d / (double)h;
+            cs[(size_t)d * h + k] = std::cos(a);
+            sn[(size_t)d * h + k] = std::sin(a);
         }
     for (int c = 0; c < 6; ++c) {
         out[c].assign((size_t)nz * plane, 0.0);
@@ -288,10 +289,10 @@ void octant_to_z_direct(int nkx, int KY, int nz, const std::vector<double> (&spe
         parallel_for(plane, [&](size_t o) {
             for (int d = 0; d < nz; ++d) {
                 double acc = 0.0;
-                for (int k = 1; k < nz; ++k)
-                    acc += S[(size_t)k * plane + o] * (oddz[c] ? sn[d * nz + k] : cs[d * nz + k]);
+                for (int k = 1; k < h; ++k)
+                    acc += S[(size_t)k * plane + o] * (oddz[c] ? sn[(size_t)d * h + k] : cs[(size_t)d * h + k]);
                 acc *= 2.0;
-                if (!oddz[c]) acc += S[o] + ((d & 1) ? -1.0 : 1.0) * S[(size_t)nz * plane + o];
+                if (!oddz[c]) acc += S[o] + ((d & 1) ? -1.0 : 1.0) * S[(size_t)h * plane + o];
                 O[(size_t)d * plane + o] = sign * acc;
             }
         });

@@ -6,7 +6,11 @@ Heun steps (inside the predictability horizon of random m0), FP32-mixed 1e-5.
 The batch pads each in-plane axis to the smallest power of two or (FP32) 3 * 2^k
 (96, 192, 384, 768) >= 2n and z to a power of two, the oracle to 2n: the fields
 agree in exact arithmetic (kernel offsets |r| <= n - 1 only).  The shapes cover
-padded lengths 16, 32, 64, 96, 128, 192, 256 and 384."""
+padded lengths 16, 32, 64, 96, 128, 192, 256 and 384.  The z convolution runs
+as the direct sum over the unpadded z (default; its table is built at the
+problem's Lz, which exceeds 2 nz for nz = 3 and 6; FP64 batches with a
+problem of nz > 4 keep the z FFT) and as the z FFT pass
+(FULLMAG_FDM_BATCH_ZCONV=fft)."""
 import numpy as np
 import pytest
 
@@ -17,7 +21,7 @@ pytestmark = pytest.mark.gpu
 
 MU0 = 4e-7 * np.pi
 SHAPES = [(37, 23, 1), (64, 32, 2), (45, 61, 3), (32, 32, 4), (100, 50, 1), (16, 128, 2), (7, 9, 3),
-          (90, 70, 2), (170, 40, 1)]
+          (90, 70, 2), (170, 40, 1), (24, 20, 6)]
 
 
 def _problems(seed=45):
@@ -44,8 +48,13 @@ def _oracle(p, dt, n):
     return sim.m
 
 
+@pytest.mark.parametrize("zconv", ["direct", "fft"])
 @pytest.mark.parametrize("precision,tol", [(nf.PRECISION_DOUBLE, 1e-10), (nf.PRECISION_SINGLE, 1e-5)])
-def test_batch_matches_oracle_per_problem(precision, tol):
+def test_batch_matches_oracle_per_problem(monkeypatch, precision, tol, zconv):
+    if zconv == "fft":
+        monkeypatch.setenv("FULLMAG_FDM_BATCH_ZCONV", "fft")
+    else:
+        monkeypatch.delenv("FULLMAG_FDM_BATCH_ZCONV", raising=False)
     probs = _problems()
     dt, n = 5e-14, 10
     with nf.NativeFdmBatch(probs, precision) as b:
