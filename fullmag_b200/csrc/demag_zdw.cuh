@@ -19,7 +19,8 @@
 // FMAs; the lower half's outputs are bitwise k_zd's, the upper half's sum each
 // pair of +d / -d terms in the other order.
 // Shared memory: 2 buffers x 64 columns x (3 nz complex + 6 nz reals),
-// 96 KiB at nz = 16: two blocks per SM.  No TMA; plain cp.async copies.
+// 96 KiB at nz = 16 (99 KiB in the window form below): two blocks per SM.
+// No TMA; plain cp.async copies.
 //
 // Window form (WIN, Ly a multiple of 128): the table is uploaded with its rows
 // padded to kyp = KY rounded up to 4 values, and a batch of 64 columns lies in
